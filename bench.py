@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Direct-space nonbonded throughput (pairs/s) on B200.
+
+Workload (default): the protein-sized synthetic system -- a 2,489-atom
+self-avoiding chain solute plus 7,023 TIP3P waters (23,558 atoms) in a
+62.23 A periodic cube, PME real space (beta 0.32) + VFSWITCH LJ, rCut 12,
+rSwitch 10, list pad 2 A rebuilt every 10 steps, FP32 coordinates moving by
+seeded Gaussian steps of 0.01 A per step.  One step = one force evaluation
+(pack + per-step recull + pair kernel + fixed-point reduction), plus the list
+rebuild on every 10th step.  pairs/s = non-excluded pairs with r < rCut (the
+oracle's count, checked against the kernel's own count) / device time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bnb|reference]
+
+--impl reference times the reference algorithm's CPU restatement (FP64
+oracle port, all host threads) on bounded samples of the same workload; the
+reference has no CPU implementation of this path.  With N>1 (torchrun) every
+rank runs its own replica (replicas only, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FLOPS_PER_PAIR = 60          # algorithmic FP32 flops per in-cutoff pair (FMA = 2)
+REBUILD_EVERY = 10
+JITTER = 0.01                # A per step
+DT_FS = 2.0
+WORKLOAD = ("chain_water_23558: 2,489-atom chain + 7,023 TIP3P, 62.23 A cube, PME(beta 0.32)+VFSWITCH, "
+            "rCut 12 rSwitch 10, pad 2 A, list rebuild every 10 steps")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="bnb", choices=["bnb", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    return ap.parse_args()
+
+
+def make_system(rank: int):
+    from blade_b200 import systems
+    s = systems.chain_in_water(seed=2 + rank)
+    return s
+
+
+def trajectory_np(s, k: int, seed: int):
+    """Frame k of the seeded jitter trajectory (CPU), FP32."""
+    rng = np.random.default_rng(seed)
+    x = s.xyz.astype(np.float64)
+    for _ in range(k):
+        x = x + rng.normal(0, JITTER, x.shape)
+    return x.astype(np.float32)
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """Samples SM clock and clock-event reasons through NVML during a region."""
+
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80}
+
+    def __init__(self, index: int):
+        self.ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.max = None
+        self.samples, self.reasons = [], set()
+        self._stop = threading.Event()
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for k, bit in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(k)
+            except Exception:
+                pass
+            time.sleep(0.005)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.ok:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max, "reasons": sorted(self.reasons), "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def ncu_traffic_per_launch():
+    """DRAM bytes per pair-kernel launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "pair_kernel_chain_water_23558.md")
+    try:
+        for line in open(path):
+            if line.strip().startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1].strip().split()[0])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# reference arm: FP64 oracle port on the host cores
+# ---------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import oracle
+    s = make_system(0)
+    cores = os.cpu_count() or 1
+    sampler = oracle.Sampler(s, nthreads=cores)
+    x = s.xyz.astype(np.float64)
+    t0 = time.perf_counter()
+    full = sampler.run(x, 0, s.N)
+    t_full = time.perf_counter() - t0
+    # window per step so that warm-up + timed steps take about a minute
+    budget = 60.0
+    frac = min(1.0, budget / max(1e-9, (args.steps + args.warmup) * t_full))
+    win = max(32, int(s.N * frac))
+    rng = np.random.default_rng(7)
+    for k in range(args.warmup):
+        i0 = (k * win) % s.N
+        sampler.run(x, i0, min(s.N, i0 + win))
+    pairs = 0
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        x = x + rng.normal(0, JITTER, x.shape)
+        i0 = ((k + args.warmup) * win) % s.N
+        pairs += sampler.run(x, i0, min(s.N, i0 + win))
+    dt = time.perf_counter() - t0
+    value = pairs / dt
+    sample = f"pairs with lower atom index in a rotating window of {win}/{s.N} atoms per step"
+    line = {"impl": "reference", "metric": "nbdirect pairs/s", "value": value, "unit": "pairs/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded chain-in-water, 23,558 atoms)",
+            "config": {"workload": WORKLOAD, "atoms": s.N, "pairs_full_eval": full},
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def run_bnb(args, rank, world):
+    import torch
+    import torch.distributed as dist
+    from blade_b200 import _lib
+    from blade_b200.nbdirect import NbDirect
+    import ctypes as C
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    s = make_system(rank)
+    K, W = args.steps, args.warmup
+    nb = NbDirect(s, device=dev)
+    stream = torch.cuda.current_stream()
+
+    # seeded trajectory, resident in HBM before timing
+    gen = torch.Generator(device=dev).manual_seed(1234 + rank)
+    x0 = torch.from_numpy(s.xyz.reshape(-1)).to(dev)
+    frames = torch.empty((K + W, 3 * s.N), dtype=torch.float32, device=dev)
+    cur = x0.double()
+    for k in range(K + W):
+        cur = cur + JITTER * torch.randn(cur.shape, generator=gen, device=dev, dtype=torch.float64)
+        frames[k] = cur.float()
+    force = torch.zeros(3 * s.N, dtype=torch.float32, device=dev)
+    energy = torch.zeros(1, dtype=torch.float64, device=dev)
+
+    def step(k, pos):
+        if k % REBUILD_EVERY == 0:
+            nb.update_domdec(pos, True, asynchronous=(k > 0))
+        nb.getforce_nbdirect(pos, None, True, force=force, energy=energy)
+
+    # warm-up (first rebuild is synchronous and sizes the list)
+    for k in range(W):
+        step(k, frames[k])
+    torch.cuda.synchronize()
+    st = nb.status(clear=True)
+    if st:
+        raise RuntimeError(f"device status {st} after warm-up")
+
+    # pair counts per step (counting pass, untimed)
+    nb.set_counting(True)
+    pairs = []
+    for k in range(W, W + K):
+        step(k - W, frames[k])
+        pairs.append(nb.pair_count())
+    nb.set_counting(False)
+    P = float(sum(pairs))
+
+    # parity on the first timed frame against the FP64 oracle (rank 0)
+    parity = None
+    if rank == 0:
+        import oracle
+        xk = frames[W].cpu().numpy().reshape(-1, 3)
+        nb.update_domdec(frames[W], True)
+        f64, _, e64 = nb.evaluate(frames[W])
+        o = oracle.nbdirect(s, xyz=xk)
+        g = f64.cpu().numpy()
+        parity = {"force_rel_rms": float(np.sqrt(((g - o["grad"]) ** 2).sum() / (o["grad"] ** 2).sum())),
+                  "energy_rel": abs(float(e64[0]) - o["energy"]) / max(abs(o["energy"]), s.N),
+                  "pairs_gpu": pairs[0], "pairs_oracle": o["pairs"]}
+
+    # L2 flush buffer (> 126 MB L2)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    nb.profile(True)
+    nb.profile_read(reset=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev.index)
+    with clocks:
+        for k in range(K):
+            flush.zero_()
+            evs[k][0].record(stream)
+            step(k, frames[W + k])
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = [a.elapsed_time(b) for a, b in evs]
+    prof = nb.profile_read(reset=True)
+    nb.profile(False)
+    st = nb.status(clear=True)
+    if st:
+        raise RuntimeError(f"device status {st} in timed region")
+    t_total = sum(ms) / 1e3
+
+    # e2e: through the C ABI with host buffers, copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        host_frames = frames.cpu().pin_memory()
+        dpos = torch.empty(3 * s.N, dtype=torch.float32, device=dev)
+        hforce = torch.empty(3 * s.N, dtype=torch.float32).pin_memory()
+        henergy = torch.empty(1, dtype=torch.float64).pin_memory()
+        e_evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+        nb.update_domdec(frames[W], True)
+        torch.cuda.synchronize()
+        for k in range(K):
+            flush.zero_()
+            e_evs[k][0].record(stream)
+            dpos.copy_(host_frames[W + k], non_blocking=True)
+            force.zero_()
+            energy.zero_()
+            step(k, dpos)
+            hforce.copy_(force, non_blocking=True)
+            henergy.copy_(energy, non_blocking=True)
+            e_evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        t_e2e = sum(a.elapsed_time(b) for a, b in e_evs) / 1e3
+        e2e = {"t": t_e2e, "h2d": 4 * 3 * s.N, "d2h": 4 * 3 * s.N + 8}
+
+    # aggregate over ranks: max time, summed pairs
+    if world > 1:
+        t = torch.tensor([t_total, e2e["t"] if e2e else 0.0], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        p = torch.tensor([P], dtype=torch.float64, device=dev)
+        dist.all_reduce(p, op=dist.ReduceOp.SUM)
+        t_total, t_e2e_max, P_all = float(t[0]), float(t[1]), float(p[0])
+    else:
+        P_all = P
+        t_e2e_max = e2e["t"] if e2e else None
+
+    if rank != 0:
+        return
+    value = P_all / t_total
+    peak = C.c_double()
+    _lib.call("bnb_fp32_peak", C.c_void_p(stream.cuda_stream), C.byref(peak))
+    pair_s = prof["pair_ms"] / 1e3
+    achieved = P * FLOPS_PER_PAIR / pair_s / 1e12
+    peak_t = peak.value / 1e12
+    traffic = ncu_traffic_per_launch()
+    line = {
+        "metric": "nbdirect pairs/s", "value": value, "unit": "pairs/s", "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": 1e3 * t_total / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded chain-in-water, 23,558 atoms per GPU)",
+        "config": {"workload": WORKLOAD, "atoms": s.N, "pairs_per_step": P / K, "jitter_A": JITTER,
+                   "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_t, "unit": "TFLOP/s",
+                     "frac": achieved / peak_t, "traffic": traffic,
+                     "kernel": "k_pair<PME,VFSWITCH> (per-launch mean over the timed region)",
+                     "flops_per_pair": FLOPS_PER_PAIR, "peak_source": "measured FP32 FMA chains (bnb_fp32_peak)",
+                     "pair_kernel_ms_mean": prof["pair_ms"] / max(1, prof["pair_launches"])},
+        "rebuild_ms_mean": prof["rebuild_ms"] / max(1, prof["rebuilds"]),
+        "ns_per_day_nbdirect_only": (K / t_total) * DT_FS * 86400 / 1e6,
+        "gpu_launches": prof["kernel_launches"],
+        "clocks": clocks.summary(),
+        "parity_vs_fp64_oracle": parity,
+    }
+    if e2e:
+        line["e2e"] = {"value": P_all / t_e2e_max, "unit": "pairs/s", "h2d_bytes_per_step": e2e["h2d"],
+                       "d2h_bytes_per_step": e2e["d2h"]}
+    if world == 1 and not args.no_cpu:
+        import oracle
+        cores = os.cpu_count() or 1
+        sam = oracle.Sampler(s, nthreads=cores)
+        x = frames[W].cpu().numpy().reshape(-1, 3).astype(np.float64)
+        n, tot, t0 = 0, 0, time.perf_counter()
+        while time.perf_counter() - t0 < args.cpu_seconds and n < 50:
+            tot += sam.run(x, 0, s.N)
+            n += 1
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": tot / dt, "unit": "pairs/s", "cores": cores, "kind": "port",
+                                "sample": f"{n} full FP64 evaluations of the first timed frame"}
+    print(json.dumps(line), flush=True)
+    nb.close()
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        if backend == "nccl":
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group(backend, timeout=timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_bnb(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

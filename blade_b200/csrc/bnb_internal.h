@@ -1,0 +1,121 @@
+// Internal device-side layout of libbnb (not part of the public C ABI).
+//
+// One handle holds R >= 1 independent systems ("replicas").  Atoms, columns,
+// blocks, candidate tiles and lambda blocks of all replicas are concatenated;
+// no block or tile ever spans two replicas.  A single system is the R == 1
+// case, so the plain and batched paths run the same kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "bnb.h"
+
+namespace bnb {
+
+constexpr int kNumShifts = 14;        // own image + 13 half-shell images
+constexpr int kTilesPerWork = 8;      // candidate tiles per pair-kernel work item
+constexpr int kMaxTableTypes = 64;    // LJ table kept in shared memory up to 64 types
+constexpr int kMaxLambdaShared = 2048;
+constexpr int kSortCap = 4096;        // column sort in shared memory up to 4096 atoms
+constexpr double kFixScale = 4294967296.0;      // 2^32 fixed-point units per kcal/mol(/A)
+constexpr float kFixScaleF = 4294967296.0f;
+
+// Status bits written by the device (bnb_status).
+enum : int {
+  kStatusBlockOverflow = BNB_STATUS_BLOCK_OVERFLOW,
+  kStatusCandOverflow = BNB_STATUS_TILE_OVERFLOW,
+  kStatusMaskOverflow = BNB_STATUS_MASK_OVERFLOW,
+  kStatusWorkOverflow = BNB_STATUS_WORK_OVERFLOW,
+  kStatusNonFinite = BNB_STATUS_NONFINITE,
+  kStatusListInvalid = BNB_STATUS_BLOCK_OVERFLOW | BNB_STATUS_TILE_OVERFLOW |
+                       BNB_STATUS_MASK_OVERFLOW | BNB_STATUS_WORK_OVERFLOW,
+};
+
+struct RepInfo {          // per replica, device copy in Dev::rep
+  float box[3];
+  int atomStart, atomCount;
+  int colStart, nCols;
+  int divX, divY;
+  int lamStart, lamCount;
+  int pad;
+};
+
+// Device-side scalar counters written by the list builder.
+struct Counters {
+  int blockCount;
+  int candCount;
+  int maskCount;
+  int workCount;
+  int status;
+  int pad[3];
+  unsigned long long pairCount;
+};
+
+struct Dev {
+  // --- static topology (set_topology) -------------------------------------
+  int N, R, nTypes, ljCombine, lamTotal;
+  RepInfo *rep;            // [R]
+  int *atomRep;            // [N]
+  float *atomQ;            // [N] charge * sqrt(kElectric)
+  int *atomType;           // [N]
+  int *atomSiteBlock;      // [N] (site<<16)|global lambda index, 0 = environment
+  float2 *ljTable;         // [nTypes*nTypes] (c12,c6)   table mode
+  float2 *ljType;          // [nTypes] (sqrt(2 eps), Rmin/2) combine mode
+  int *exclStart;          // [N+1]
+  int *exclAtom;           // [E]
+  // --- capacities ----------------------------------------------------------
+  int totalCols, maxBlocks, capCand, capMask, capWork;
+  // --- rebuild products ----------------------------------------------------
+  int *wrap;               // [N] packed integer image shift
+  int *atomCol;            // [N]
+  uint32_t *atomZKey;      // [N]
+  int *colCount;           // [totalCols]
+  int *colStartAtom;       // [totalCols+1]
+  int *colStartBlock;      // [totalCols+1]
+  int *colFill;            // [totalCols]
+  int *bucket;             // [N]
+  int *sortedAtom;         // [N]
+  int *blockBounds;        // [maxBlocks+1]
+  int *blockRep;           // [maxBlocks]
+  int *repBlockStart;      // [R+1]
+  int *slotAtom;           // [32*maxBlocks]
+  int *atomSlot;           // [N]
+  float *slotQ;            // [32*maxBlocks]
+  int *slotType;           // [32*maxBlocks]
+  int *slotSiteBlock;      // [32*maxBlocks]
+  int *cullCount;          // [maxBlocks*kNumShifts]
+  int *cullOffset;         // [maxBlocks*kNumShifts+1]
+  int4 *cand;              // [capCand] (jBlock, shiftCode, maskIdx, iBlock)
+  int *candFlag;           // [capCand]
+  int *candMaskOff;        // [capCand+1]
+  uint32_t *masks;         // [capMask*32]
+  int *candStart;          // [maxBlocks+1]
+  int *workCountPerBlock;  // [maxBlocks]
+  int *workOffset;         // [maxBlocks+1]
+  int2 *work;              // [capWork] (iBlock, candidate start)
+  int *scanPartial;        // scratch for multi-CTA scans
+  // --- per-step buffers -----------------------------------------------------
+  float4 *xyzq;            // [32*maxBlocks]
+  float4 *bmin, *bmax;     // [maxBlocks]
+  long long *accF;         // [3*32*maxBlocks] SoA fixed-point dU/dx per slot
+  long long *accL;         // [lamTotal]
+  long long *accE;         // [1]
+  Counters *ctr;
+};
+
+struct PairConst {        // uniform parameters of the pair kernel
+  float rc2, rcut, rswitch, beta;
+  float softR;            // soft-core radius (4 A in AKMA)
+  // PME
+  float mBeta2Log2e;      // -beta^2 * log2(e)
+  float twoBetaSqrtPi;    // 2*beta/sqrt(pi)
+  // VFSWITCH
+  float k6, k12, rci3, rci6, dv6, dv12;
+  // VSWITCH / VSHIFT / FSWITCH / FSHIFT helpers
+  float roff2, ron2, rul3inv, rul12;
+  float fA, fB, fC, fD, fdvc, rcinv;
+  float vshRc6inv, vshRc12inv, vshRc18inv;
+};
+
+}  // namespace bnb

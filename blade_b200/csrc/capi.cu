@@ -1,0 +1,747 @@
+// C ABI of libbnb: handle life cycle, topology upload, list rebuild with
+// capacity growth, and the per-step direct-space evaluation.
+//
+// Host-side counterpart of Domdec::initialize/reset_domdec/update_domdec
+// (src/domdec/domdec.cu:83-222) and getforce_nbdirect
+// (src/nbdirect/nbdirect.cu:492-581).  All device memory of a handle lives in
+// two arenas (topology, list); capacities grow only inside a synchronous
+// rebuild, never during an asynchronous (graph-capturable) call.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "bnb.h"
+#include "bnb_internal.h"
+#include "listbuild.h"
+#include "nbdirect.h"
+
+using bnb::Dev;
+using bnb::PairConst;
+using bnb::RepInfo;
+
+struct bnb_handle {
+  bnb_params p;
+  int R = 0, N = 0;
+  std::vector<int> atomCount, atomStart;
+  // topology
+  bool topo = false;
+  int nTypes = 0, combine = 0, lamTotal = 0, alch = 0;
+  std::vector<int> lamStart, lamCount;
+  size_t exclTotal = 0;
+  // columns / replicas
+  std::vector<RepInfo> rep;
+  std::vector<int> colRep;
+  int totalCols = 0;
+  // capacities
+  int maxBlocks = 0, capCand = 0, capMask = 0, capWork = 0;
+  bool listBuilt = false;
+  int lastWork = 0;
+  int resTiles = 0, resMasks = 0, resWork = 0;
+  bool reserveDirty = false;
+  bool counting = false;
+  // profiling (bnb_profile)
+  bool prof = false;
+  std::vector<cudaEvent_t> pairEv, rebEv;
+  int pairN = 0, rebN = 0;
+  unsigned long long launches = 0;
+  // device
+  Dev d{};
+  void *topoArena = nullptr, *listArena = nullptr;
+  size_t listBytes = 0;
+  int *colRep_d = nullptr;
+  PairConst pc{};
+};
+
+namespace {
+
+// Largest list capacity: the three-pass scan handles up to 4096 x 4096 items.
+constexpr long long kCapLimit = 4096LL * 4096LL;
+constexpr int kProfSlots = 4096;
+
+void destroy_events(bnb_handle *h) {
+  for (auto e : h->pairEv) cudaEventDestroy(e);
+  for (auto e : h->rebEv) cudaEventDestroy(e);
+  h->pairEv.clear();
+  h->rebEv.clear();
+  h->pairN = h->rebN = 0;
+}
+
+struct Arena {
+  size_t off = 0;
+  template <typename T>
+  size_t take(size_t n) {
+    size_t o = off;
+    off += ((sizeof(T) * (n > 0 ? n : 1)) + 255) & ~size_t(255);
+    return o;
+  }
+};
+
+inline bool ok(cudaError_t e) { return e == cudaSuccess; }
+
+PairConst make_const(const bnb_params &p) {
+  PairConst c{};
+  double rc = p.rCut, rs = p.rSwitch, b = p.betaEwald;
+  c.rcut = (float)rc;
+  c.rswitch = (float)rs;
+  c.rc2 = (float)rc * (float)rc;
+  c.beta = (float)b;
+  c.softR = p.softCoreRadius;
+  c.mBeta2Log2e = (float)(-b * b / std::log(2.0));
+  c.twoBetaSqrtPi = (float)(2.0 * b / std::sqrt(M_PI));
+  double rc3 = rc * rc * rc, rs3 = rs * rs * rs;
+  c.k6 = (float)(rc3 / (rc3 - rs3));
+  c.k12 = (float)(rc3 * rc3 / (rc3 * rc3 - rs3 * rs3));
+  c.rci3 = (float)(1.0 / rc3);
+  c.rci6 = (float)(1.0 / (rc3 * rc3));
+  double dv6 = 1.0 / (rc3 * rs3);
+  c.dv6 = (float)dv6;
+  c.dv12 = (float)(dv6 * dv6);
+  double roff2 = rc * rc, ron2 = rs * rs;
+  c.roff2 = (float)roff2;
+  c.ron2 = (float)ron2;
+  double rul3 = (roff2 - ron2) * (roff2 - ron2) * (roff2 - ron2);
+  c.rul3inv = (float)(1.0 / rul3);
+  c.rul12 = (float)(12.0 / rul3);
+  double ginv = 1.0 / rul3;
+  c.fA = (float)(roff2 * roff2 * (roff2 - 3 * ron2) * ginv);
+  c.fB = (float)(6 * roff2 * ron2 * ginv);
+  c.fC = (float)(-(ron2 + roff2) * ginv);
+  c.fD = (float)(2 * ginv / 5);
+  c.fdvc = (float)(8 * (ron2 * roff2 * (rc - rs) - (roff2 * roff2 * rc - ron2 * ron2 * rs) / 5) * ginv);
+  c.rcinv = (float)(1.0 / rc);
+  double rc6 = roff2 * roff2 * roff2;
+  c.vshRc6inv = (float)(1.0 / rc6);
+  c.vshRc12inv = (float)(1.0 / (rc6 * rc6));
+  c.vshRc18inv = (float)(1.0 / (rc6 * rc6 * rc6));
+  return c;
+}
+
+void free_list(bnb_handle *h) {
+  if (h->listArena) cudaFree(h->listArena);
+  h->listArena = nullptr;
+  h->listBytes = 0;
+  h->listBuilt = false;
+}
+
+// (Re)allocates the list arena for the current capacities.
+int alloc_list(bnb_handle *h) {
+  free_list(h);
+  Dev &d = h->d;
+  const int N = h->N, C = h->totalCols, MB = h->maxBlocks;
+  Arena a;
+  size_t o_wrap = a.take<int>(N), o_col = a.take<int>(N), o_z = a.take<uint32_t>(N);
+  size_t o_cc = a.take<int>(C), o_csa = a.take<int>(C + 1), o_csb = a.take<int>(C + 1),
+         o_cf = a.take<int>(C), o_colrep = a.take<int>(C);
+  size_t o_bucket = a.take<int>(N), o_sorted = a.take<int>(N);
+  size_t o_bb = a.take<int>(MB + 1), o_brep = a.take<int>(MB), o_rbs = a.take<int>(h->R + 1);
+  size_t o_slotA = a.take<int>(32 * MB), o_atomSlot = a.take<int>(N), o_slotQ = a.take<float>(32 * MB),
+         o_slotT = a.take<int>(32 * MB), o_slotSB = a.take<int>(32 * MB);
+  size_t o_cullC = a.take<int>(MB * bnb::kNumShifts), o_cullO = a.take<int>(MB * bnb::kNumShifts + 1);
+  size_t o_cand = a.take<int4>(h->capCand), o_cflag = a.take<int>(h->capCand),
+         o_cmo = a.take<int>(h->capCand + 1);
+  size_t o_masks = a.take<uint32_t>(32 * (size_t)h->capMask);
+  size_t o_cs = a.take<int>(MB + 1), o_wcb = a.take<int>(MB), o_wo = a.take<int>(MB + 1),
+         o_work = a.take<int2>(h->capWork);
+  size_t o_part = a.take<int>(4096);
+  size_t o_xyzq = a.take<float4>(32 * MB), o_bmin = a.take<float4>(MB), o_bmax = a.take<float4>(MB);
+  size_t o_acc = a.take<long long>(3 * 32 * (size_t)MB);
+  void *base = nullptr;
+  if (!ok(cudaMalloc(&base, a.off))) return BNB_ERR_CUDA;
+  h->listArena = base;
+  h->listBytes = a.off;
+  char *b = static_cast<char *>(base);
+  d.wrap = (int *)(b + o_wrap);
+  d.atomCol = (int *)(b + o_col);
+  d.atomZKey = (uint32_t *)(b + o_z);
+  d.colCount = (int *)(b + o_cc);
+  d.colStartAtom = (int *)(b + o_csa);
+  d.colStartBlock = (int *)(b + o_csb);
+  d.colFill = (int *)(b + o_cf);
+  h->colRep_d = (int *)(b + o_colrep);
+  d.bucket = (int *)(b + o_bucket);
+  d.sortedAtom = (int *)(b + o_sorted);
+  d.blockBounds = (int *)(b + o_bb);
+  d.blockRep = (int *)(b + o_brep);
+  d.repBlockStart = (int *)(b + o_rbs);
+  d.slotAtom = (int *)(b + o_slotA);
+  d.atomSlot = (int *)(b + o_atomSlot);
+  d.slotQ = (float *)(b + o_slotQ);
+  d.slotType = (int *)(b + o_slotT);
+  d.slotSiteBlock = (int *)(b + o_slotSB);
+  d.cullCount = (int *)(b + o_cullC);
+  d.cullOffset = (int *)(b + o_cullO);
+  d.cand = (int4 *)(b + o_cand);
+  d.candFlag = (int *)(b + o_cflag);
+  d.candMaskOff = (int *)(b + o_cmo);
+  d.masks = (uint32_t *)(b + o_masks);
+  d.candStart = (int *)(b + o_cs);
+  d.workCountPerBlock = (int *)(b + o_wcb);
+  d.workOffset = (int *)(b + o_wo);
+  d.work = (int2 *)(b + o_work);
+  d.scanPartial = (int *)(b + o_part);
+  d.xyzq = (float4 *)(b + o_xyzq);
+  d.bmin = (float4 *)(b + o_bmin);
+  d.bmax = (float4 *)(b + o_bmax);
+  d.accF = (long long *)(b + o_acc);
+  d.totalCols = C;
+  d.maxBlocks = MB;
+  d.capCand = h->capCand;
+  d.capMask = h->capMask;
+  d.capWork = h->capWork;
+  if (!ok(cudaMemset(base, 0, a.off))) return BNB_ERR_CUDA;
+  if (!ok(cudaMemcpy(h->colRep_d, h->colRep.data(), sizeof(int) * std::max(C, 1),
+                     cudaMemcpyHostToDevice)))
+    return BNB_ERR_CUDA;
+  return BNB_OK;
+}
+
+// Column grid per replica from its box; returns true if the layout changed.
+bool layout_columns(bnb_handle *h, const float *boxes) {
+  bool changed = false;
+  int col = 0;
+  std::vector<int> colRep;
+  for (int r = 0; r < h->R; r++) {
+    RepInfo &ri = h->rep[r];
+    int dx, dy;
+    bnb_domain_div(h->atomCount[r], boxes + 3 * r, &dx, &dy);
+    if (dx != ri.divX || dy != ri.divY || col != ri.colStart) changed = true;
+    ri.divX = dx;
+    ri.divY = dy;
+    ri.colStart = col;
+    ri.nCols = dx * dy;
+    for (int k = 0; k < 3; k++) ri.box[k] = boxes[3 * r + k];
+    for (int c = 0; c < ri.nCols; c++) colRep.push_back(r);
+    col += ri.nCols;
+  }
+  h->totalCols = col;
+  h->colRep.swap(colRep);
+  return changed;
+}
+
+void estimate_capacities(bnb_handle *h, int &mb, long long &cand, long long &work, long long &mask) {
+  mb = 0;
+  cand = 0;
+  for (int r = 0; r < h->R; r++) {
+    const RepInfo &ri = h->rep[r];
+    int n = h->atomCount[r];
+    int blocks = n / 32 + ri.nCols + 1;
+    mb += blocks;
+    if (n == 0) continue;
+    double vol = (double)ri.box[0] * ri.box[1] * ri.box[2];
+    double invDens = vol / n;
+    double approx = std::cbrt(32 * invDens);
+    double edge = approx + 2.0 * (h->p.rCut + h->p.cullPad);
+    double perBlock = 0.75 * edge * edge * edge / (32 * invDens) + 16;
+    cand += (long long)(perBlock * (n / 32 + 1)) + 14;
+  }
+  work = cand / bnb::kTilesPerWork + mb + 16;
+  mask = (long long)(4 * h->exclTotal + 1024) / 32 + 64;
+}
+
+int upload_rep(bnb_handle *h, cudaStream_t s) {
+  for (int r = 0; r < h->R; r++) {
+    h->rep[r].atomStart = h->atomStart[r];
+    h->rep[r].atomCount = h->atomCount[r];
+    h->rep[r].lamStart = h->lamStart.empty() ? 0 : h->lamStart[r];
+    h->rep[r].lamCount = h->lamCount.empty() ? 1 : h->lamCount[r];
+  }
+  return ok(cudaMemcpyAsync(h->d.rep, h->rep.data(), sizeof(RepInfo) * h->R,
+                            cudaMemcpyHostToDevice, s))
+             ? BNB_OK
+             : BNB_ERR_CUDA;
+}
+
+__global__ void k_clear_list_status(bnb::Counters *c) {
+  atomicAnd(&c->status, ~bnb::kStatusListInvalid);
+}
+
+}  // namespace
+
+extern "C" {
+
+void bnb_default_params(bnb_params *p) {
+  if (!p) return;
+  p->rCut = 12.0f;
+  p->rSwitch = 10.0f;
+  p->betaEwald = 0.32f;
+  p->elecMethod = 1;
+  p->vdwMethod = 0;
+  p->useSoftCore = 1;
+  p->cullPad = 2.0f;
+  p->kElectric = 332.0716f;
+  p->softCoreRadius = 4.0f;
+}
+
+const char *bnb_version(void) { return "bnb 0.1 (sm_100a)"; }
+
+int bnb_domain_div(int atomCount, const float *box, int *divX, int *divY) {
+  if (!box || !divX || !divY || atomCount < 0) return BNB_ERR_ARG;
+  if (atomCount == 0) {
+    *divX = *divY = 1;
+    return BNB_OK;
+  }
+  // Same FP32 steps as Domdec::initialize, src/domdec/domdec.cu:114-117.
+  float invDensity = box[0] * box[1] * box[2] / (float)atomCount;
+  float approx = expf(logf(32.0f * invDensity) / 3.0f);
+  int x = (int)ceilf(box[0] / approx), y = (int)ceilf(box[1] / approx);
+  *divX = x < 1 ? 1 : x;
+  *divY = y < 1 ? 1 : y;
+  return BNB_OK;
+}
+
+int bnb_create(const bnb_params *p, int replicas, const int *atomCounts, bnb_handle **out) {
+  if (!p || !out || replicas < 1 || !atomCounts) return BNB_ERR_ARG;
+  if (p->elecMethod < 0 || p->elecMethod > 2 || p->vdwMethod < 0 || p->vdwMethod > 2) return BNB_ERR_ARG;
+  if (!(p->rCut > 0) || !(p->rSwitch > 0) || p->rSwitch > p->rCut || p->cullPad < 0) return BNB_ERR_ARG;
+  bnb_handle *h = new (std::nothrow) bnb_handle();
+  if (!h) return BNB_ERR_ARG;
+  h->p = *p;
+  h->R = replicas;
+  h->atomCount.assign(atomCounts, atomCounts + replicas);
+  h->atomStart.resize(replicas + 1);
+  h->atomStart[0] = 0;
+  for (int r = 0; r < replicas; r++) {
+    if (atomCounts[r] < 0) { delete h; return BNB_ERR_ARG; }
+    h->atomStart[r + 1] = h->atomStart[r] + atomCounts[r];
+  }
+  h->N = h->atomStart[replicas];
+  h->rep.assign(replicas, RepInfo{});
+  for (auto &r : h->rep) { r.divX = -1; r.divY = -1; r.colStart = -1; }
+  h->pc = make_const(*p);
+  *out = h;
+  return BNB_OK;
+}
+
+int bnb_destroy(bnb_handle *h) {
+  if (!h) return BNB_ERR_ARG;
+  free_list(h);
+  if (h->topoArena) cudaFree(h->topoArena);
+  destroy_events(h);
+  delete h;
+  return BNB_OK;
+}
+
+int bnb_set_topology(bnb_handle *h, const bnb_nbond *nbonds, const int *typeCounts,
+                     const bnb_vdw *vdw, const int *lambdaCounts, int exclCount, const int *excl,
+                     const int *exclReplica) {
+  if (!h || (h->N > 0 && !nbonds) || !typeCounts || !vdw || exclCount < 0 ||
+      (exclCount > 0 && !excl) || (exclCount > 0 && h->R > 1 && !exclReplica))
+    return BNB_ERR_ARG;
+  const int R = h->R, N = h->N;
+  std::vector<int> typeStart(R + 1, 0);
+  for (int r = 0; r < R; r++) {
+    if (typeCounts[r] < 1) return BNB_ERR_ARG;
+    typeStart[r + 1] = typeStart[r] + typeCounts[r];
+  }
+  const int T = typeStart[R];
+  h->lamStart.assign(R, 0);
+  h->lamCount.assign(R, 1);
+  int lam = 0;
+  h->alch = 0;
+  for (int r = 0; r < R; r++) {
+    int c = lambdaCounts ? lambdaCounts[r] : 1;
+    if (c < 1) return BNB_ERR_ARG;
+    h->lamStart[r] = lam;
+    h->lamCount[r] = c;
+    if (c > 1) h->alch = 1;
+    lam += c;
+  }
+  if (lam > bnb::kMaxLambdaShared || lam >= 65536) return BNB_ERR_UNSUPPORTED;
+  h->lamTotal = lam;
+
+  // Per-atom arrays.
+  std::vector<int> atomRep(N), atomType(N), atomSB(N);
+  std::vector<float> atomQ(N);
+  const float sk = std::sqrt(h->p.kElectric);
+  for (int r = 0; r < R; r++)
+    for (int a = h->atomStart[r]; a < h->atomStart[r + 1]; a++) {
+      const bnb_nbond nb = nbonds[a];
+      if (nb.typeIdx < 0 || nb.typeIdx >= typeCounts[r]) return BNB_ERR_ARG;
+      atomRep[a] = r;
+      atomType[a] = typeStart[r] + nb.typeIdx;
+      atomQ[a] = nb.q * sk;
+      int blk = nb.siteBlock & 0xFFFF, site = (nb.siteBlock >> 16) & 0xFFFF;
+      if (nb.siteBlock == 0) {
+        atomSB[a] = 0;
+      } else {
+        if (blk >= h->lamCount[r] || blk == 0) return BNB_ERR_ARG;
+        atomSB[a] = (site << 16) | (h->lamStart[r] + blk);
+      }
+    }
+
+  // LJ: shared-memory table when small, otherwise per-type combination
+  // parameters (requires the table to follow the combination rule of
+  // potential.cxx:1393-1403, i.e. no NBFIX overrides).
+  h->nTypes = T;
+  h->combine = T > bnb::kMaxTableTypes ? 1 : 0;
+  std::vector<float2> table, ljType;
+  if (!h->combine) {
+    table.assign((size_t)T * T, make_float2(0.f, 0.f));
+    size_t off = 0;
+    for (int r = 0; r < R; r++) {
+      int t = typeCounts[r];
+      for (int i = 0; i < t; i++)
+        for (int j = 0; j < t; j++) {
+          bnb_vdw v = vdw[off + (size_t)i * t + j];
+          table[(size_t)(typeStart[r] + i) * T + typeStart[r] + j] = make_float2(v.c12, v.c6);
+        }
+      off += (size_t)t * t;
+    }
+  } else {
+    ljType.resize(T);
+    size_t off = 0;
+    for (int r = 0; r < R; r++) {
+      int t = typeCounts[r];
+      std::vector<double> e(t), rh(t);
+      for (int i = 0; i < t; i++) {
+        bnb_vdw v = vdw[off + (size_t)i * t + i];
+        if (v.c6 > 0 && v.c12 > 0) {
+          double R6 = 2.0 * v.c12 / v.c6;      // (2 Rmin/2)^6
+          e[i] = (double)v.c6 * v.c6 / (4.0 * v.c12);
+          rh[i] = 0.5 * std::pow(R6, 1.0 / 6.0);
+        } else {
+          e[i] = 0;
+          rh[i] = 0;
+        }
+      }
+      for (int i = 0; i < t; i++)
+        for (int j = 0; j < t; j++) {
+          bnb_vdw v = vdw[off + (size_t)i * t + j];
+          double eps = std::sqrt(e[i] * e[j]), Rm = rh[i] + rh[j];
+          double c6 = 2 * eps * std::pow(Rm, 6), c12 = eps * std::pow(Rm, 12);
+          if (std::fabs(c6 - v.c6) > 1e-4 * std::fabs(c6) + 1e-12 ||
+              std::fabs(c12 - v.c12) > 1e-4 * std::fabs(c12) + 1e-12)
+            return BNB_ERR_UNSUPPORTED;
+        }
+      for (int i = 0; i < t; i++)
+        ljType[typeStart[r] + i] = make_float2((float)std::sqrt(2.0 * e[i]), (float)rh[i]);
+      off += (size_t)t * t;
+    }
+  }
+
+  // Exclusions -> per-atom CSR over global indices (sorted, no duplicates).
+  std::vector<std::pair<int, int>> ex;
+  ex.reserve(exclCount);
+  for (int e = 0; e < exclCount; e++) {
+    int r = h->R > 1 ? exclReplica[e] : 0;
+    if (r < 0 || r >= R) return BNB_ERR_ARG;
+    int a = excl[2 * e], b = excl[2 * e + 1];
+    if (a < 0 || b < 0 || a >= h->atomCount[r] || b >= h->atomCount[r]) return BNB_ERR_ARG;
+    a += h->atomStart[r];
+    b += h->atomStart[r];
+    if (a == b) continue;
+    ex.emplace_back(a, b);
+    ex.emplace_back(b, a);
+  }
+  std::sort(ex.begin(), ex.end());
+  ex.erase(std::unique(ex.begin(), ex.end()), ex.end());
+  std::vector<int> exStart(N + 1, 0), exAtom(ex.size());
+  for (auto &pr : ex) exStart[pr.first + 1]++;
+  for (int a = 0; a < N; a++) exStart[a + 1] += exStart[a];
+  for (size_t k = 0; k < ex.size(); k++) exAtom[k] = ex[k].second;
+  h->exclTotal = ex.size();
+
+  // Upload into the topology arena.
+  if (h->topoArena) cudaFree(h->topoArena);
+  h->topoArena = nullptr;
+  Arena a;
+  size_t o_rep = a.take<RepInfo>(R), o_arep = a.take<int>(N), o_q = a.take<float>(N),
+         o_t = a.take<int>(N), o_sb = a.take<int>(N),
+         o_tab = a.take<float2>(h->combine ? 1 : (size_t)T * T),
+         o_lt = a.take<float2>(h->combine ? T : 1), o_es = a.take<int>(N + 1),
+         o_ea = a.take<int>(ex.size()), o_accL = a.take<long long>(lam), o_accE = a.take<long long>(R),
+         o_ctr = a.take<bnb::Counters>(1);
+  void *base = nullptr;
+  if (!ok(cudaMalloc(&base, a.off))) return BNB_ERR_CUDA;
+  h->topoArena = base;
+  char *b = static_cast<char *>(base);
+  Dev &d = h->d;
+  d.N = N;
+  d.R = R;
+  d.nTypes = T;
+  d.ljCombine = h->combine;
+  d.lamTotal = lam;
+  d.rep = (RepInfo *)(b + o_rep);
+  d.atomRep = (int *)(b + o_arep);
+  d.atomQ = (float *)(b + o_q);
+  d.atomType = (int *)(b + o_t);
+  d.atomSiteBlock = (int *)(b + o_sb);
+  d.ljTable = (float2 *)(b + o_tab);
+  d.ljType = (float2 *)(b + o_lt);
+  d.exclStart = (int *)(b + o_es);
+  d.exclAtom = (int *)(b + o_ea);
+  d.accL = (long long *)(b + o_accL);
+  d.accE = (long long *)(b + o_accE);
+  d.ctr = (bnb::Counters *)(b + o_ctr);
+  bool good = ok(cudaMemset(base, 0, a.off));
+  auto up = [&](void *dst, const void *src, size_t n) {
+    if (n) good = good && ok(cudaMemcpy(dst, src, n, cudaMemcpyHostToDevice));
+  };
+  up(d.atomRep, atomRep.data(), sizeof(int) * N);
+  up(d.atomQ, atomQ.data(), sizeof(float) * N);
+  up(d.atomType, atomType.data(), sizeof(int) * N);
+  up(d.atomSiteBlock, atomSB.data(), sizeof(int) * N);
+  if (!h->combine) up(d.ljTable, table.data(), sizeof(float2) * table.size());
+  else up(d.ljType, ljType.data(), sizeof(float2) * ljType.size());
+  up(d.exclStart, exStart.data(), sizeof(int) * (N + 1));
+  up(d.exclAtom, exAtom.data(), sizeof(int) * exAtom.size());
+  if (!good) return BNB_ERR_CUDA;
+  h->topo = true;
+  free_list(h);  // any previous list refers to the old topology
+  for (auto &r : h->rep) { r.divX = -1; r.divY = -1; r.colStart = -1; }
+  return BNB_OK;
+}
+
+int bnb_rebuild(bnb_handle *h, const float *position, const float *boxes, void *stream, int flags) {
+  if (!h || !boxes || (h->N > 0 && !position)) return BNB_ERR_ARG;
+  if (!h->topo) return BNB_ERR_STATE;
+  for (int r = 0; r < h->R; r++)
+    for (int k = 0; k < 3; k++) {
+      float L = boxes[3 * r + k];
+      if (!(L >= 2 * h->p.rCut)) return BNB_ERR_ARG;  // single-image scheme needs rCut <= box/2
+    }
+  cudaStream_t s = (cudaStream_t)stream;
+  const bool async = (flags & BNB_ASYNC) != 0;
+  bool changed = layout_columns(h, boxes);
+  int mb;
+  long long cand, work, mask;
+  estimate_capacities(h, mb, cand, work, mask);
+  bool need = !h->listArena || mb > h->maxBlocks || h->totalCols != h->d.totalCols || changed ||
+              h->reserveDirty;
+  if (need) {
+    if (async && !h->reserveDirty) return BNB_ERR_STATE;  // sizes change only in a synchronous rebuild
+    cudaStreamSynchronize(s);
+    h->maxBlocks = std::max(mb, h->maxBlocks);
+    h->capCand = h->resTiles > 0 ? h->resTiles
+                                 : (int)std::max<long long>(h->capCand, std::min<long long>(cand, kCapLimit));
+    h->capWork = h->resWork > 0 ? h->resWork
+                                : (int)std::max<long long>(h->capWork, std::min<long long>(work, kCapLimit));
+    h->capMask = h->resMasks > 0 ? h->resMasks : (int)std::max<long long>(h->capMask, mask);
+    h->reserveDirty = false;
+    int rc = alloc_list(h);
+    if (rc) return rc;
+  }
+  int rc = upload_rep(h, s);
+  if (rc) return rc;
+  const float rcull = h->p.rCut + h->p.cullPad;
+  const float rcull2 = rcull * rcull;
+  for (int attempt = 0; attempt < 12; attempt++) {
+    const bool rec = h->prof && h->rebN < kProfSlots;
+    if (rec) cudaEventRecord(h->rebEv[2 * h->rebN], s);
+    k_clear_list_status<<<1, 1, 0, s>>>(h->d.ctr);
+    h->launches += 1 + bnb::rebuild_list(h->d, h->colRep_d, position, rcull2, s);
+    if (rec) cudaEventRecord(h->rebEv[2 * h->rebN++ + 1], s);
+    if (!ok(cudaGetLastError())) return BNB_ERR_CUDA;
+    if (async) {
+      h->listBuilt = true;
+      return BNB_OK;
+    }
+    bnb::Counters c;
+    if (!ok(cudaMemcpyAsync(&c, h->d.ctr, sizeof(c), cudaMemcpyDeviceToHost, s))) return BNB_ERR_CUDA;
+    if (!ok(cudaStreamSynchronize(s))) return BNB_ERR_CUDA;
+    int bad = c.status & bnb::kStatusListInvalid;
+    if (!bad) {
+      h->listBuilt = true;
+      h->lastWork = c.workCount;
+      return BNB_OK;
+    }
+    if (bad & bnb::kStatusBlockOverflow) return BNB_ERR_CAPACITY;  // cannot happen by construction
+    // Grow what overflowed by 1.5x (src/domdec/cull.cu:337-375) and retry.
+    int needCand = 0;
+    if (bad & bnb::kStatusCandOverflow) {
+      cudaMemcpy(&needCand, h->d.cullOffset + h->maxBlocks * bnb::kNumShifts, sizeof(int),
+                 cudaMemcpyDeviceToHost);
+      h->capCand = (int)std::min<long long>((long long)std::max(needCand, h->capCand) * 3 / 2, kCapLimit);
+      h->capWork = std::max(h->capWork, h->capCand / bnb::kTilesPerWork + h->maxBlocks + 16);
+    }
+    if (bad & bnb::kStatusMaskOverflow) {
+      int needMask = 0;
+      cudaMemcpy(&needMask, h->d.candMaskOff + h->d.capCand, sizeof(int), cudaMemcpyDeviceToHost);
+      h->capMask = std::max(needMask, h->capMask) * 3 / 2 + 64;
+    }
+    if (bad & bnb::kStatusWorkOverflow) h->capWork = h->capWork * 3 / 2 + 64;
+    rc = alloc_list(h);
+    if (rc) return rc;
+    rc = upload_rep(h, s);
+    if (rc) return rc;
+  }
+  return BNB_ERR_CAPACITY;
+}
+
+int bnb_compute(bnb_handle *h, const float *position, const float *lambda, const float *boxes,
+                int calcEnergy, const bnb_outputs *out, void *stream) {
+  if (!h || !out || !boxes || (h->N > 0 && !position)) return BNB_ERR_ARG;
+  if (!h->listBuilt) return BNB_ERR_STATE;
+  if (h->alch && !lambda) return BNB_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  bool boxChanged = false;
+  for (int r = 0; r < h->R; r++)
+    for (int k = 0; k < 3; k++)
+      if (h->rep[r].box[k] != boxes[3 * r + k]) {
+        h->rep[r].box[k] = boxes[3 * r + k];
+        boxChanged = true;
+      }
+  if (boxChanged) {
+    int rc = upload_rep(h, s);
+    if (rc) return rc;
+  }
+  if (h->counting) cudaMemsetAsync(&h->d.ctr->pairCount, 0, sizeof(unsigned long long), s);
+  bnb::pack_positions(h->d, position, s);
+  int alch = h->alch ? (h->p.useSoftCore ? 2 : 1) : 0;
+  int work = h->lastWork > 0 ? h->lastWork : h->capWork;
+  int grid = (work + 7) / 8;
+  grid = std::max(1, std::min(grid, 148 * 8));
+  const bool rec = h->prof && h->pairN < kProfSlots;
+  if (rec) cudaEventRecord(h->pairEv[2 * h->pairN], s);
+  int rc = bnb::launch_pair(h->d, h->pc, lambda, h->p.elecMethod, h->p.vdwMethod, alch,
+                            calcEnergy != 0, h->counting, grid, s);
+  if (rec) cudaEventRecord(h->pairEv[2 * h->pairN++ + 1], s);
+  if (rc) return rc;
+  bnb::launch_finalize(h->d, *out, s);
+  h->launches += 3;
+  return ok(cudaGetLastError()) ? BNB_OK : BNB_ERR_CUDA;
+}
+
+int bnb_profile(bnb_handle *h, int enable) {
+  if (!h) return BNB_ERR_ARG;
+  if (enable && h->pairEv.empty()) {
+    h->pairEv.resize(2 * kProfSlots);
+    h->rebEv.resize(2 * kProfSlots);
+    for (auto &e : h->pairEv)
+      if (!ok(cudaEventCreate(&e))) return BNB_ERR_CUDA;
+    for (auto &e : h->rebEv)
+      if (!ok(cudaEventCreate(&e))) return BNB_ERR_CUDA;
+  }
+  h->prof = enable != 0;
+  h->pairN = h->rebN = 0;
+  return BNB_OK;
+}
+
+int bnb_profile_read(bnb_handle *h, double *pairMs, int *pairLaunches, double *rebuildMs,
+                     int *rebuilds, unsigned long long *kernelLaunches, int reset) {
+  if (!h) return BNB_ERR_ARG;
+  double pm = 0, rm = 0;
+  for (int i = 0; i < h->pairN; i++) {
+    float ms = 0;
+    if (!ok(cudaEventSynchronize(h->pairEv[2 * i + 1])) ||
+        !ok(cudaEventElapsedTime(&ms, h->pairEv[2 * i], h->pairEv[2 * i + 1])))
+      return BNB_ERR_CUDA;
+    pm += ms;
+  }
+  for (int i = 0; i < h->rebN; i++) {
+    float ms = 0;
+    if (!ok(cudaEventSynchronize(h->rebEv[2 * i + 1])) ||
+        !ok(cudaEventElapsedTime(&ms, h->rebEv[2 * i], h->rebEv[2 * i + 1])))
+      return BNB_ERR_CUDA;
+    rm += ms;
+  }
+  if (pairMs) *pairMs = pm;
+  if (pairLaunches) *pairLaunches = h->pairN;
+  if (rebuildMs) *rebuildMs = rm;
+  if (rebuilds) *rebuilds = h->rebN;
+  if (kernelLaunches) *kernelLaunches = h->launches;
+  if (reset) {
+    h->pairN = h->rebN = 0;
+    h->launches = 0;
+  }
+  return BNB_OK;
+}
+
+int bnb_reserve(bnb_handle *h, int tiles, int masks, int work) {
+  if (!h) return BNB_ERR_ARG;
+  h->resTiles = tiles > 0 ? tiles : 0;
+  h->resMasks = masks > 0 ? masks : 0;
+  h->resWork = work > 0 ? work : 0;
+  h->reserveDirty = true;
+  return BNB_OK;
+}
+
+int bnb_status(bnb_handle *h, void *stream, int clear, int *status) {
+  if (!h || !status) return BNB_ERR_ARG;
+  if (!h->topo) { *status = 0; return BNB_OK; }
+  cudaStream_t s = (cudaStream_t)stream;
+  int v = 0;
+  if (!ok(cudaMemcpyAsync(&v, &h->d.ctr->status, sizeof(int), cudaMemcpyDeviceToHost, s)) ||
+      !ok(cudaStreamSynchronize(s)))
+    return BNB_ERR_CUDA;
+  if (clear) cudaMemsetAsync(&h->d.ctr->status, 0, sizeof(int), s);
+  *status = v;
+  return BNB_OK;
+}
+
+int bnb_list_sizes(bnb_handle *h, void *stream, int *blocks, int *tiles, int *masks, int *work) {
+  if (!h) return BNB_ERR_ARG;
+  if (!h->listBuilt) return BNB_ERR_STATE;
+  bnb::Counters c;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!ok(cudaMemcpyAsync(&c, h->d.ctr, sizeof(c), cudaMemcpyDeviceToHost, s)) ||
+      !ok(cudaStreamSynchronize(s)))
+    return BNB_ERR_CUDA;
+  if (blocks) *blocks = c.blockCount;
+  if (tiles) *tiles = c.candCount;
+  if (masks) *masks = c.maskCount;
+  if (work) *work = c.workCount;
+  return BNB_OK;
+}
+
+int bnb_get_list(bnb_handle *h, void *stream, int *wrap, int *blockBounds, int *sortedAtom,
+                 int *slotAtom, float *bmin, float *bmax, int *candStart, int *cand, int *candMask,
+                 uint32_t *masks) {
+  int B, T, M, W;
+  int rc = bnb_list_sizes(h, stream, &B, &T, &M, &W);
+  if (rc) return rc;
+  const Dev &d = h->d;
+  bool good = true;
+  auto dn = [&](void *dst, const void *src, size_t n) {
+    if (dst && n) good = good && ok(cudaMemcpy(dst, src, n, cudaMemcpyDeviceToHost));
+  };
+  dn(wrap, d.wrap, sizeof(int) * h->N);
+  dn(blockBounds, d.blockBounds, sizeof(int) * (B + 1));
+  dn(sortedAtom, d.sortedAtom, sizeof(int) * h->N);
+  dn(slotAtom, d.slotAtom, sizeof(int) * 32 * B);
+  if (bmin || bmax) {
+    std::vector<float4> t(B > 0 ? B : 1);
+    if (bmin) {
+      dn(t.data(), d.bmin, sizeof(float4) * B);
+      for (int b = 0; b < B; b++) { bmin[3 * b] = t[b].x; bmin[3 * b + 1] = t[b].y; bmin[3 * b + 2] = t[b].z; }
+    }
+    if (bmax) {
+      dn(t.data(), d.bmax, sizeof(float4) * B);
+      for (int b = 0; b < B; b++) { bmax[3 * b] = t[b].x; bmax[3 * b + 1] = t[b].y; bmax[3 * b + 2] = t[b].z; }
+    }
+  }
+  dn(candStart, d.candStart, sizeof(int) * (B + 1));
+  if (cand || candMask) {
+    std::vector<int4> t(T > 0 ? T : 1);
+    dn(t.data(), d.cand, sizeof(int4) * T);
+    for (int c = 0; c < T; c++) {
+      if (cand) { cand[2 * c] = t[c].x; cand[2 * c + 1] = t[c].y; }
+      if (candMask) candMask[c] = t[c].z;
+    }
+  }
+  dn(masks, d.masks, sizeof(uint32_t) * 32 * (size_t)M);
+  return good ? BNB_OK : BNB_ERR_CUDA;
+}
+
+int bnb_set_counting(bnb_handle *h, int enable) {
+  if (!h) return BNB_ERR_ARG;
+  h->counting = enable != 0;
+  return BNB_OK;
+}
+
+int bnb_pair_count(bnb_handle *h, void *stream, unsigned long long *pairs) {
+  if (!h || !pairs) return BNB_ERR_ARG;
+  if (!h->topo) return BNB_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!ok(cudaMemcpyAsync(pairs, &h->d.ctr->pairCount, sizeof(*pairs), cudaMemcpyDeviceToHost, s)) ||
+      !ok(cudaStreamSynchronize(s)))
+    return BNB_ERR_CUDA;
+  return BNB_OK;
+}
+
+}  // extern "C"

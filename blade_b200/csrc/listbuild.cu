@@ -1,0 +1,564 @@
+// Block neighbour-list builder for the direct-space path (sm_100a).
+//
+// Counterpart of the reference's Domdec::reset_domdec
+// (src/domdec/domdec.cu:201-211): bin atoms into x/y columns
+// (assign_blocks.cu:24-60), order each column by z (assign_blocks.cu:62-178),
+// cut columns into blocks of <=32 atoms (assign_blocks.cu:189-308), build
+// AABBs (assign_blocks.cu:340-382), cull block pairs over the 14-image half
+// shell at rCut+pad (cull.cu:44-299) and attach 32x32 exclusion masks
+// (assign_excl.cu:17-313).  Differences by design:
+//   * deterministic: z ties broken by atom index; all compactions are
+//     order-preserving scans, so the list is identical run to run;
+//   * no host synchronisation: counts stay on the device and capacity
+//     overflow raises a status bit instead of a host readback;
+//   * batched: R replicas in one pass, tiles never cross replicas.
+// Every FP32 step is one IEEE operation (__f*_rn, built with -fmad=false),
+// the sequence restated on the CPU in oracle/listbuild_oracle.c.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "bnb_internal.h"
+#include "listbuild.h"
+
+namespace bnb {
+
+namespace {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+__device__ __forceinline__ uint32_t z_key(float z) {
+  uint32_t u = __float_as_uint(z);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__device__ __forceinline__ int shift_code_vec(int code, int *sx, int *sy) {
+  // Half shell of cull.cu:127-173: z in {0,1}; y in {-z..1};
+  // x in {-(y!=0||z!=0)..1}.  Codes enumerate that loop in order.
+  // code: 0,1 -> (0..1,0,0); 2..4 -> (-1..1,1,0); 5..13 -> (-1..1,-1..1,1)
+  int x, y, z;
+  if (code < 2) { x = code; y = 0; z = 0; }
+  else if (code < 5) { x = code - 3; y = 1; z = 0; }
+  else { int c = code - 5; x = c % 3 - 1; y = c / 3 - 1; z = 1; }
+  *sx = x; *sy = y;
+  return z;
+}
+
+// AABB gap^2 <= c2 with the operation order of orc_aabb_hit.
+__device__ __forceinline__ bool aabb_hit(float4 imin, float4 imax, float4 jmin,
+                                         float4 jmax, float3 sh, float c2) {
+  float lo, hi, g1, g2, g, acc;
+  lo = __fadd_rn(jmin.x, sh.x); hi = __fadd_rn(jmax.x, sh.x);
+  g1 = __fsub_rn(lo, imax.x); g2 = __fsub_rn(imin.x, hi);
+  g = g1 > g2 ? g1 : g2; g = g > 0.0f ? g : 0.0f;
+  acc = __fmul_rn(g, g);
+  lo = __fadd_rn(jmin.y, sh.y); hi = __fadd_rn(jmax.y, sh.y);
+  g1 = __fsub_rn(lo, imax.y); g2 = __fsub_rn(imin.y, hi);
+  g = g1 > g2 ? g1 : g2; g = g > 0.0f ? g : 0.0f;
+  acc = __fadd_rn(acc, __fmul_rn(g, g));
+  lo = __fadd_rn(jmin.z, sh.z); hi = __fadd_rn(jmax.z, sh.z);
+  g1 = __fsub_rn(lo, imax.z); g2 = __fsub_rn(imin.z, hi);
+  g = g1 > g2 ? g1 : g2; g = g > 0.0f ? g : 0.0f;
+  acc = __fadd_rn(acc, __fmul_rn(g, g));
+  return acc <= c2;
+}
+
+// ---------------------------------------------------------------------------
+// Exclusive scan over int arrays (three passes, 4096 items per CTA).
+// ---------------------------------------------------------------------------
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ int block_excl_scan(int v, int *total) {
+  __shared__ int warpSums[kScanThreads / 32];
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(kFull, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warpSums[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int s = lane < kScanThreads / 32 ? warpSums[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(kFull, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < kScanThreads / 32) warpSums[lane] = s;
+  }
+  __syncthreads();
+  int before = w > 0 ? warpSums[w - 1] : 0;
+  *total = warpSums[kScanThreads / 32 - 1];
+  __syncthreads();
+  return before + x - v;
+}
+
+__global__ void k_scan_reduce(const int *in, int n, int *partial) {
+  int base = blockIdx.x * kScanTile;
+  int s = 0;
+  for (int i = threadIdx.x; i < kScanTile; i += kScanThreads) {
+    int k = base + i;
+    if (k < n) s += in[k];
+  }
+  int tot;
+  block_excl_scan(s, &tot);
+  if (threadIdx.x == 0) partial[blockIdx.x] = tot;
+}
+
+__global__ void k_scan_top(int *partial, int nParts, int *total) {
+  // nParts <= kScanTile
+  int v[kScanItems];
+  int s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    int i = threadIdx.x * kScanItems + k;
+    v[k] = i < nParts ? partial[i] : 0;
+    s += v[k];
+  }
+  int tot;
+  int off = block_excl_scan(s, &tot);
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    int i = threadIdx.x * kScanItems + k;
+    if (i < nParts) partial[i] = off;
+    off += v[k];
+  }
+  if (threadIdx.x == 0 && total) *total = tot;
+}
+
+__global__ void k_scan_down(const int *in, int *out, int n, const int *partial) {
+  int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  int v[kScanItems];
+  int s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    int i = base + k;
+    v[k] = i < n ? in[i] : 0;
+    s += v[k];
+  }
+  int tot;
+  int off = block_excl_scan(s, &tot) + partial[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    int i = base + k;
+    if (i < n) out[i] = off;
+    off += v[k];
+  }
+}
+
+}  // namespace
+
+void scan_exclusive(const int *in, int *out, int n, int *total, int *partial,
+                    cudaStream_t s) {
+  int parts = (n + kScanTile - 1) / kScanTile;
+  if (parts < 1) parts = 1;
+  k_scan_reduce<<<parts, kScanThreads, 0, s>>>(in, n, partial);
+  k_scan_top<<<1, kScanThreads, 0, s>>>(partial, parts, total);
+  k_scan_down<<<parts, kScanThreads, 0, s>>>(in, out, n, partial);
+}
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// 1. Binning: wrap shift, column and z key per atom.
+// ---------------------------------------------------------------------------
+__global__ void k_bin(Dev d, const float *__restrict__ pos) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= d.N) return;
+  const RepInfo ri = d.rep[d.atomRep[a]];
+  float w[3];
+  int s[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    float x = pos[3 * a + k];
+    if (!isfinite(x)) atomicOr(&d.ctr->status, kStatusNonFinite);
+    float L = ri.box[k];
+    float f = floorf(__fdiv_rn(x, L));
+    f = fminf(fmaxf(f, -127.0f), 127.0f);
+    s[k] = (int)f;
+    w[k] = __fsub_rn(x, __fmul_rn(f, L));
+  }
+  d.wrap[a] = (s[0] + 128) | ((s[1] + 128) << 8) | ((s[2] + 128) << 16);
+  int ix = (int)floorf(__fmul_rn(__fdiv_rn(w[0], ri.box[0]), (float)ri.divX));
+  ix = ix >= ri.divX ? ri.divX - 1 : ix;
+  ix = ix < 0 ? 0 : ix;
+  int iy = (int)floorf(__fmul_rn(__fdiv_rn(w[1], ri.box[1]), (float)ri.divY));
+  iy = iy >= ri.divY ? ri.divY - 1 : iy;
+  iy = iy < 0 ? 0 : iy;
+  int col = ri.colStart + ix * ri.divY + iy;
+  d.atomCol[a] = col;
+  d.atomZKey[a] = z_key(w[2]);
+  atomicAdd(&d.colCount[col], 1);
+}
+
+// ---------------------------------------------------------------------------
+// 2. Column scan (single CTA): atom offsets, block offsets, block bounds.
+// ---------------------------------------------------------------------------
+__global__ void k_colscan(Dev d, const int *__restrict__ colRep) {
+  __shared__ int carryA, carryB;
+  if (threadIdx.x == 0) { carryA = 0; carryB = 0; }
+  __syncthreads();
+  const int nc = d.totalCols;
+  for (int c0 = 0; c0 < nc; c0 += blockDim.x) {
+    int c = c0 + threadIdx.x;
+    int n = c < nc ? d.colCount[c] : 0;
+    int nb = (n + 31) >> 5;
+    // two block-wide scans via warp shuffles and shared memory
+    __shared__ int wa[32], wb[32];
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int xa = n, xb = nb;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int ya = __shfl_up_sync(kFull, xa, o), yb = __shfl_up_sync(kFull, xb, o);
+      if (lane >= o) { xa += ya; xb += yb; }
+    }
+    if (lane == 31) { wa[w] = xa; wb[w] = xb; }
+    __syncthreads();
+    if (w == 0) {
+      int sa = lane < nw ? wa[lane] : 0, sb = lane < nw ? wb[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int ya = __shfl_up_sync(kFull, sa, o), yb = __shfl_up_sync(kFull, sb, o);
+        if (lane >= o) { sa += ya; sb += yb; }
+      }
+      if (lane < nw) { wa[lane] = sa; wb[lane] = sb; }
+    }
+    __syncthreads();
+    int offA = carryA + (w ? wa[w - 1] : 0) + xa - n;
+    int offB = carryB + (w ? wb[w - 1] : 0) + xb - nb;
+    if (c < nc) {
+      d.colStartAtom[c] = offA;
+      d.colStartBlock[c] = offB;
+      d.colFill[c] = 0;
+      int r = colRep[c];
+      for (int k = 0; k < nb; k++) {
+        int b = offB + k;
+        if (b < d.maxBlocks) {
+          d.blockBounds[b] = offA + 32 * k;
+          d.blockRep[b] = r;
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) { carryA += wa[nw - 1]; carryB += wb[nw - 1]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    int B = carryB;
+    d.colStartAtom[nc] = carryA;
+    d.colStartBlock[nc] = B;
+    if (B > d.maxBlocks) {
+      atomicOr(&d.ctr->status, kStatusBlockOverflow);
+      B = d.maxBlocks;
+    }
+    d.blockBounds[B] = carryA;
+    d.ctr->blockCount = B;
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r <= d.R; r += blockDim.x) {
+    int b = r < d.R ? d.colStartBlock[d.rep[r].colStart] : d.colStartBlock[nc];
+    d.repBlockStart[r] = b < d.maxBlocks ? b : d.maxBlocks;
+  }
+}
+
+// 3. Scatter atoms into column buckets (arbitrary order within a column).
+__global__ void k_scatter(Dev d) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= d.N) return;
+  int col = d.atomCol[a];
+  int p = d.colStartAtom[col] + atomicAdd(&d.colFill[col], 1);
+  d.bucket[p] = a;
+}
+
+// 4. Sort each column by (z key, atom index): bitonic sort in shared memory,
+//    rank counting for columns larger than kSortCap.
+__global__ void k_colsort(Dev d) {
+  __shared__ unsigned long long key[kSortCap];
+  const int c = blockIdx.x;
+  const int n = d.colCount[c];
+  const int base = d.colStartAtom[c];
+  if (n == 0) return;
+  if (n <= kSortCap) {
+    int n2 = 1;
+    while (n2 < n) n2 <<= 1;
+    for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+      if (i < n) {
+        int a = d.bucket[base + i];
+        key[i] = ((unsigned long long)d.atomZKey[a] << 32) | (unsigned)a;
+      } else {
+        key[i] = ~0ull;
+      }
+    }
+    __syncthreads();
+    for (int k = 2; k <= n2; k <<= 1) {
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+          int ixj = i ^ j;
+          if (ixj > i) {
+            unsigned long long x = key[i], y = key[ixj];
+            bool up = (i & k) == 0;
+            if ((x > y) == up) { key[i] = y; key[ixj] = x; }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+      d.sortedAtom[base + i] = (int)(key[i] & 0xFFFFFFFFull);
+  } else {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      int a = d.bucket[base + i];
+      unsigned long long ki = ((unsigned long long)d.atomZKey[a] << 32) | (unsigned)a;
+      int rank = 0;
+      for (int j = 0; j < n; j++) {
+        int b = d.bucket[base + j];
+        unsigned long long kj = ((unsigned long long)d.atomZKey[b] << 32) | (unsigned)b;
+        rank += kj < ki;
+      }
+      d.sortedAtom[base + rank] = a;
+    }
+  }
+}
+
+// 5. Slots: atom of each of the 32 lanes of each block, per-slot parameters.
+__global__ void k_slots(Dev d) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int b = t >> 5, lane = t & 31;
+  if (b >= d.maxBlocks) return;
+  int B = d.ctr->blockCount;
+  if (b >= B) return;
+  int i0 = d.blockBounds[b], i1 = d.blockBounds[b + 1];
+  int idx = i0 + lane;
+  // a block never extends past its column: bounds of the next block start a
+  // new column or lie 32 further in the same column
+  int end = i0 + 32 < i1 ? i0 + 32 : i1;
+  if (idx < end) {
+    int a = d.sortedAtom[idx];
+    d.slotAtom[t] = a;
+    d.atomSlot[a] = t;
+    d.slotQ[t] = d.atomQ[a];
+    d.slotType[t] = d.atomType[a];
+    d.slotSiteBlock[t] = d.atomSiteBlock[a];
+  } else {
+    d.slotAtom[t] = -1;
+    d.slotQ[t] = 0.0f;
+    d.slotType[t] = 0;
+    d.slotSiteBlock[t] = 0;
+  }
+}
+
+}  // namespace
+
+// 6. Pack coordinates with the stored image shift; per-block AABBs.
+__global__ void k_pack(Dev d, const float *__restrict__ pos) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int b = t >> 5;
+  if (b >= d.maxBlocks) return;
+  if (b >= d.ctr->blockCount) return;
+  int a = d.slotAtom[t];
+  const RepInfo &ri = d.rep[d.blockRep[b]];
+  float3 p = make_float3(0.f, 0.f, 0.f);
+  float3 mn = make_float3(INFINITY, INFINITY, INFINITY);
+  float3 mx = make_float3(-INFINITY, -INFINITY, -INFINITY);
+  if (a >= 0) {
+    int w = d.wrap[a];
+    float sx = (float)((w & 0xFF) - 128), sy = (float)(((w >> 8) & 0xFF) - 128),
+          sz = (float)(((w >> 16) & 0xFF) - 128);
+    p.x = __fsub_rn(pos[3 * a], __fmul_rn(sx, ri.box[0]));
+    p.y = __fsub_rn(pos[3 * a + 1], __fmul_rn(sy, ri.box[1]));
+    p.z = __fsub_rn(pos[3 * a + 2], __fmul_rn(sz, ri.box[2]));
+    mn = p;
+    mx = p;
+  }
+  d.xyzq[t] = make_float4(p.x, p.y, p.z, d.slotQ[t]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mn.x = fminf(mn.x, __shfl_xor_sync(kFull, mn.x, o));
+    mn.y = fminf(mn.y, __shfl_xor_sync(kFull, mn.y, o));
+    mn.z = fminf(mn.z, __shfl_xor_sync(kFull, mn.z, o));
+    mx.x = fmaxf(mx.x, __shfl_xor_sync(kFull, mx.x, o));
+    mx.y = fmaxf(mx.y, __shfl_xor_sync(kFull, mx.y, o));
+    mx.z = fmaxf(mx.z, __shfl_xor_sync(kFull, mx.z, o));
+  }
+  if ((t & 31) == 0) {
+    d.bmin[b] = make_float4(mn.x, mn.y, mn.z, 0.f);
+    d.bmax[b] = make_float4(mx.x, mx.y, mx.z, 0.f);
+  }
+}
+
+namespace {
+
+// 7/9. Cull: one warp per (iBlock, shift code); count pass then write pass.
+template <bool kWrite>
+__global__ void k_cull(Dev d, float rcull2) {
+  const int lane = threadIdx.x & 31;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  const int B = d.ctr->blockCount;
+  const int total = d.maxBlocks * kNumShifts;
+  for (int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gw < total; gw += nWarps) {
+    int iBlock = gw / kNumShifts, code = gw - iBlock * kNumShifts;
+    if (iBlock >= B) {
+      if (!kWrite && lane == 0) d.cullCount[gw] = 0;
+      continue;
+    }
+    int r = d.blockRep[iBlock];
+    const RepInfo &ri = d.rep[r];
+    int sx, sy, sz = shift_code_vec(code, &sx, &sy);
+    float3 sh = make_float3(__fmul_rn((float)sx, ri.box[0]), __fmul_rn((float)sy, ri.box[1]),
+                            __fmul_rn((float)sz, ri.box[2]));
+    float4 imin = d.bmin[iBlock], imax = d.bmax[iBlock];
+    int j0 = code == 0 ? iBlock : d.repBlockStart[r];
+    int j1 = d.repBlockStart[r + 1];
+    int cnt = 0;
+    int base = kWrite ? d.cullOffset[gw] : 0;
+    for (int jb = j0; jb < j1; jb += 32) {
+      int j = jb + lane;
+      bool hit = false;
+      if (j < j1) hit = aabb_hit(imin, imax, d.bmin[j], d.bmax[j], sh, rcull2);
+      unsigned m = __ballot_sync(kFull, hit);
+      if (kWrite && hit) {
+        int p = base + cnt + __popc(m & ((1u << lane) - 1u));
+        if (p < d.capCand) d.cand[p] = make_int4(j, code, -1, iBlock);
+      }
+      cnt += __popc(m);
+    }
+    if (!kWrite && lane == 0) d.cullCount[gw] = cnt;
+  }
+}
+
+// Candidate bookkeeping after the cull scan.
+__global__ void k_cand_finish(Dev d) {
+  int total = d.cullOffset[d.maxBlocks * kNumShifts];
+  int B = d.ctr->blockCount;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) {
+    d.ctr->candCount = total < d.capCand ? total : d.capCand;
+    if (total > d.capCand) atomicOr(&d.ctr->status, kStatusCandOverflow);
+  }
+  for (int b = t; b <= B; b += gridDim.x * blockDim.x) {
+    int s = d.cullOffset[b * kNumShifts];
+    d.candStart[b] = s < d.capCand ? s : d.capCand;
+    if (b < B) {
+      int e = d.cullOffset[(b + 1) * kNumShifts];
+      e = e < d.capCand ? e : d.capCand;
+      s = s < d.capCand ? s : d.capCand;
+      d.workCountPerBlock[b] = (e - s + kTilesPerWork - 1) / kTilesPerWork;
+    }
+  }
+  for (int b = B + t; b < d.maxBlocks; b += gridDim.x * blockDim.x) d.workCountPerBlock[b] = 0;
+}
+
+// 10/12. Exclusion rows of a candidate tile: one warp, lane = i atom.
+__device__ __forceinline__ uint32_t excl_row(const Dev &d, int iBlock, int jBlock, int lane) {
+  uint32_t row = 0xFFFFFFFFu;
+  int a = d.slotAtom[32 * iBlock + lane];
+  if (a >= 0) {
+    int e1 = d.exclStart[a + 1];
+    for (int e = d.exclStart[a]; e < e1; e++) {
+      int b = d.exclAtom[e];
+      if (b == a) continue;
+      int sl = d.atomSlot[b];
+      if ((sl >> 5) == jBlock) row &= ~(1u << (sl & 31));
+    }
+  }
+  return row;
+}
+
+template <bool kWrite>
+__global__ void k_excl(Dev d) {
+  const int lane = threadIdx.x & 31;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  const int n = d.ctr->candCount;
+  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < d.capCand; c += nWarps) {
+    if (c >= n) {
+      if (!kWrite && lane == 0) d.candFlag[c] = 0;
+      continue;
+    }
+    int4 t = d.cand[c];
+    uint32_t row = excl_row(d, t.w, t.x, lane);
+    bool any = __any_sync(kFull, row != 0xFFFFFFFFu);
+    if (!kWrite) {
+      if (lane == 0) d.candFlag[c] = any ? 1 : 0;
+    } else {
+      int idx = -1;
+      if (any) {
+        idx = d.candMaskOff[c];
+        if (idx < d.capMask) d.masks[32 * (size_t)idx + lane] = row;
+        else idx = -1;
+      }
+      if (lane == 0) d.cand[c].z = idx;
+    }
+  }
+}
+
+__global__ void k_mask_finish(Dev d) {
+  int total = d.candMaskOff[d.capCand];
+  d.ctr->maskCount = total < d.capMask ? total : d.capMask;
+  if (total > d.capMask) atomicOr(&d.ctr->status, kStatusMaskOverflow);
+}
+
+// 13. Work items: (iBlock, first candidate) chunks of kTilesPerWork tiles.
+__global__ void k_work(Dev d) {
+  const int B = d.ctr->blockCount;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) {
+    int total = d.workOffset[d.maxBlocks];
+    d.ctr->workCount = total < d.capWork ? total : d.capWork;
+    if (total > d.capWork) atomicOr(&d.ctr->status, kStatusWorkOverflow);
+  }
+  for (int b = t; b < B; b += gridDim.x * blockDim.x) {
+    int w0 = d.workOffset[b], nw = d.workCountPerBlock[b];
+    int s = d.candStart[b];
+    for (int k = 0; k < nw; k++)
+      if (w0 + k < d.capWork) d.work[w0 + k] = make_int2(b, s + k * kTilesPerWork);
+  }
+}
+
+inline int grid_for(long long n, int threads) {
+  long long g = (n + threads - 1) / threads;
+  if (g < 1) g = 1;
+  if (g > 65535LL * 16) g = 65535LL * 16;
+  return (int)g;
+}
+
+}  // namespace
+
+void pack_positions(const Dev &d, const float *pos, cudaStream_t s) {
+  int n = 32 * d.maxBlocks;
+  k_pack<<<grid_for(n, 256), 256, 0, s>>>(d, pos);
+}
+
+int rebuild_list(const Dev &d, const int *colRep, const float *pos, float rcull2,
+                 cudaStream_t s) {
+  cudaMemsetAsync(d.colCount, 0, sizeof(int) * d.totalCols, s);
+  const int launches = (d.N > 0 ? 2 : 0) + 20;
+  if (d.N > 0) k_bin<<<grid_for(d.N, 256), 256, 0, s>>>(d, pos);
+  k_colscan<<<1, 1024, 0, s>>>(d, colRep);
+  if (d.N > 0) k_scatter<<<grid_for(d.N, 256), 256, 0, s>>>(d);
+  k_colsort<<<d.totalCols, 512, 0, s>>>(d);
+  k_slots<<<grid_for(32LL * d.maxBlocks, 256), 256, 0, s>>>(d);
+  pack_positions(d, pos, s);
+  // cull: count, scan, write
+  const int cullWarps = d.maxBlocks * kNumShifts;
+  const int cullGrid = grid_for(32LL * cullWarps, 256) < 148 * 32 ? grid_for(32LL * cullWarps, 256) : 148 * 32;
+  k_cull<false><<<cullGrid, 256, 0, s>>>(d, rcull2);
+  scan_exclusive(d.cullCount, d.cullOffset, cullWarps, d.cullOffset + cullWarps, d.scanPartial, s);
+  k_cull<true><<<cullGrid, 256, 0, s>>>(d, rcull2);
+  k_cand_finish<<<grid_for(d.maxBlocks + 1, 256), 256, 0, s>>>(d);
+  // exclusion masks: flag, scan, write
+  const int exGrid = grid_for(32LL * d.capCand, 256) < 148 * 16 ? grid_for(32LL * d.capCand, 256) : 148 * 16;
+  k_excl<false><<<exGrid, 256, 0, s>>>(d);
+  scan_exclusive(d.candFlag, d.candMaskOff, d.capCand, d.candMaskOff + d.capCand, d.scanPartial, s);
+  k_excl<true><<<exGrid, 256, 0, s>>>(d);
+  k_mask_finish<<<1, 1, 0, s>>>(d);
+  // work items
+  scan_exclusive(d.workCountPerBlock, d.workOffset, d.maxBlocks, d.workOffset + d.maxBlocks,
+                 d.scanPartial, s);
+  k_work<<<grid_for(d.maxBlocks, 256), 256, 0, s>>>(d);
+  return launches;
+}
+
+}  // namespace bnb

@@ -1,0 +1,202 @@
+"""Host side of the direct-space path: the Domdec / getforce_nbdirect mirror.
+
+``NbDirect`` owns one libbnb handle for one system or a batch of replicas and
+exposes the reference's calling surface for this path:
+
+* ``update_domdec(positions, reset)``  -- Domdec::update_domdec
+  (src/domdec/domdec.cu:213-222): ``reset=True`` rebuilds the block list
+  (reset_domdec), otherwise nothing happens until the next force call.
+* ``getforce_nbdirect(positions, lambdas, calc_energy, ...)`` -- the entry
+  point of src/nbdirect/nbdirect.cu:574: pack, recull, pair kernel, unpack.
+  Like the reference, outputs are accumulated into caller buffers (dU/dx in
+  ``force``, dU/dlambda in ``lambda_force``, energy in ``energy``); the exact
+  fixed-point totals are also available as FP64 (``force64`` etc.).
+
+Device memory and streams come from torch (plumbing only); every kernel is
+in libbnb.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+from .systems import NBOND_DTYPE, System
+
+
+def _ptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def _stream(stream):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def params_for(sys: System) -> _lib.Params:
+    p = _lib.Params()
+    _lib.lib().bnb_default_params(C.byref(p))
+    p.rCut, p.rSwitch, p.betaEwald = sys.rCut, sys.rSwitch, sys.betaEwald
+    p.elecMethod, p.vdwMethod = sys.elecMethod, sys.vdwMethod
+    p.useSoftCore = int(bool(sys.msld and sys.msld.useSoftCore))
+    p.cullPad = sys.cullPad
+    return p
+
+
+class NbDirect:
+    """One handle over ``systems`` (a System or a list of replicas)."""
+
+    def __init__(self, systems: System | Sequence[System], device=None):
+        import torch
+        self.systems = [systems] if isinstance(systems, System) else list(systems)
+        s0 = self.systems[0]
+        for s in self.systems[1:]:
+            if (s.rCut, s.rSwitch, s.betaEwald, s.elecMethod, s.vdwMethod, s.cullPad) != \
+               (s0.rCut, s0.rSwitch, s0.betaEwald, s0.elecMethod, s0.vdwMethod, s0.cullPad):
+                raise ValueError("replicas of one handle share cutoffs and methods")
+        self.device = torch.device(device if device is not None else "cuda")
+        self.R = len(self.systems)
+        self.counts = np.array([s.N for s in self.systems], np.int32)
+        self.starts = np.concatenate([[0], np.cumsum(self.counts)]).astype(np.int64)
+        self.N = int(self.starts[-1])
+        self.lam_counts = np.array([s.msld.blockCount if s.msld else 1 for s in self.systems], np.int32)
+        self.lam_starts = np.concatenate([[0], np.cumsum(self.lam_counts)]).astype(np.int64)
+        self.L = int(self.lam_starts[-1])
+        self.params = params_for(s0)
+        self.params.useSoftCore = int(any(bool(s.msld and s.msld.useSoftCore) for s in self.systems))
+        h = C.c_void_p()
+        _lib.call("bnb_create", C.byref(self.params), self.R, self.counts.ctypes.data_as(C.c_void_p), C.byref(h))
+        self.h = h
+        self._set_topology()
+        self.boxes = np.concatenate([np.asarray(s.box, np.float32) for s in self.systems]).astype(np.float32)
+
+    # -- topology --------------------------------------------------------------
+    def _set_topology(self):
+        nb = np.ascontiguousarray(np.concatenate([s.nbonds for s in self.systems]).astype(NBOND_DTYPE))
+        types = np.array([s.nTypes for s in self.systems], np.int32)
+        vdw = np.ascontiguousarray(np.concatenate([s.vdw.reshape(-1, 2) for s in self.systems]), np.float32)
+        excl = [s.excl.astype(np.int32) for s in self.systems]
+        exr = np.ascontiguousarray(np.concatenate([np.full(len(e), r, np.int32) for r, e in enumerate(excl)]))
+        ex = np.ascontiguousarray(np.concatenate(excl) if excl else np.zeros((0, 2), np.int32))
+        _lib.call("bnb_set_topology", self.h, nb.ctypes.data_as(C.c_void_p), types.ctypes.data_as(C.c_void_p),
+                  vdw.ctypes.data_as(C.c_void_p), self.lam_counts.ctypes.data_as(C.c_void_p), len(ex),
+                  ex.ctypes.data_as(C.c_void_p), exr.ctypes.data_as(C.c_void_p))
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.lib().bnb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- reference calling surface ---------------------------------------------
+    def update_domdec(self, positions, reset: bool, stream=None, asynchronous: bool = False,
+                      boxes=None):
+        """Domdec::update_domdec: rebuild the list when ``reset`` is true."""
+        if not reset:
+            return
+        b = np.ascontiguousarray(self.boxes if boxes is None else boxes, np.float32)
+        _lib.call("bnb_rebuild", self.h, _ptr(positions), b.ctypes.data_as(C.c_void_p), _stream(stream),
+                  _lib.BNB_ASYNC if asynchronous else 0)
+
+    reset_domdec = lambda self, positions, stream=None: self.update_domdec(positions, True, stream)
+
+    def getforce_nbdirect(self, positions, lambdas=None, calc_energy=True, force=None,
+                          lambda_force=None, energy=None, force64=None, lambda_force64=None,
+                          energy64=None, stream=None, boxes=None):
+        out = _lib.Outputs(force=_ptr(force), lambdaForce=_ptr(lambda_force), energy=_ptr(energy),
+                           force64=_ptr(force64), lambdaForce64=_ptr(lambda_force64), energy64=_ptr(energy64))
+        b = np.ascontiguousarray(self.boxes if boxes is None else boxes, np.float32)
+        _lib.call("bnb_compute", self.h, _ptr(positions), _ptr(lambdas), b.ctypes.data_as(C.c_void_p),
+                  int(bool(calc_energy)), C.byref(out), _stream(stream))
+
+    # -- conveniences ------------------------------------------------------------
+    def positions_tensor(self, xyz_list=None):
+        import torch
+        xs = xyz_list if xyz_list is not None else [s.xyz for s in self.systems]
+        return torch.from_numpy(np.ascontiguousarray(np.concatenate(xs), np.float32)).to(self.device).reshape(-1)
+
+    def lambdas_tensor(self, lam_list=None):
+        import torch
+        ls = lam_list if lam_list is not None else [s.lambdas() for s in self.systems]
+        return torch.from_numpy(np.concatenate(ls).astype(np.float32)).to(self.device)
+
+    def evaluate(self, positions=None, lambdas=None, calc_energy=True, stream=None):
+        """One evaluation with fresh FP64 outputs: (force64 [N,3], dU/dlambda [L], energy [R])."""
+        import torch
+        pos = self.positions_tensor() if positions is None else positions
+        lam = self.lambdas_tensor() if lambdas is None else lambdas
+        f64 = torch.zeros(3 * self.N, dtype=torch.float64, device=self.device)
+        l64 = torch.zeros(self.L, dtype=torch.float64, device=self.device)
+        e64 = torch.zeros(self.R, dtype=torch.float64, device=self.device)
+        self.getforce_nbdirect(pos, lam, calc_energy, force64=f64, lambda_force64=l64, energy64=e64,
+                               stream=stream)
+        return f64.reshape(-1, 3), l64, e64
+
+    def status(self, clear=False, stream=None) -> int:
+        v = C.c_int()
+        _lib.call("bnb_status", self.h, _stream(stream), int(clear), C.byref(v))
+        return v.value
+
+    def reserve(self, tiles=0, masks=0, work=0):
+        """Preset list capacities before the next rebuild (bnb_reserve)."""
+        _lib.call("bnb_reserve", self.h, int(tiles), int(masks), int(work))
+
+    def profile(self, on: bool):
+        """Record CUDA events around the pair kernel and list rebuilds."""
+        _lib.call("bnb_profile", self.h, int(on))
+
+    def profile_read(self, reset=True):
+        pm, rm = C.c_double(), C.c_double()
+        pn, rn = C.c_int(), C.c_int()
+        kl = C.c_ulonglong()
+        _lib.call("bnb_profile_read", self.h, C.byref(pm), C.byref(pn), C.byref(rm), C.byref(rn),
+                  C.byref(kl), int(reset))
+        return {"pair_ms": pm.value, "pair_launches": pn.value, "rebuild_ms": rm.value,
+                "rebuilds": rn.value, "kernel_launches": kl.value}
+
+    def set_counting(self, on: bool):
+        _lib.call("bnb_set_counting", self.h, int(on))
+
+    def pair_count(self, stream=None) -> int:
+        v = C.c_ulonglong()
+        _lib.call("bnb_pair_count", self.h, _stream(stream), C.byref(v))
+        return v.value
+
+    def list_sizes(self, stream=None):
+        v = [C.c_int() for _ in range(4)]
+        _lib.call("bnb_list_sizes", self.h, _stream(stream), *[C.byref(x) for x in v])
+        return {"blocks": v[0].value, "tiles": v[1].value, "masks": v[2].value, "work": v[3].value}
+
+    def get_list(self, stream=None):
+        sz = self.list_sizes(stream)
+        B, T, M = sz["blocks"], sz["tiles"], sz["masks"]
+        wrap = np.zeros(self.N, np.int32)
+        bb = np.zeros(B + 1, np.int32)
+        sa = np.zeros(self.N, np.int32)
+        slot = np.zeros(32 * B, np.int32)
+        bmin = np.zeros((B, 3), np.float32)
+        bmax = np.zeros((B, 3), np.float32)
+        cs = np.zeros(B + 1, np.int32)
+        cand = np.zeros((T, 2), np.int32)
+        cm = np.zeros(T, np.int32)
+        masks = np.zeros((M, 32), np.uint32)
+        P = lambda a: a.ctypes.data_as(C.c_void_p)
+        _lib.call("bnb_get_list", self.h, _stream(stream), P(wrap), P(bb), P(sa), P(slot), P(bmin), P(bmax),
+                  P(cs), P(cand), P(cm), P(masks))
+        return {"blockCount": B, "wrap": wrap, "blockBounds": bb, "sortedAtom": sa, "slotAtom": slot,
+                "bmin": bmin, "bmax": bmax, "candStart": cs, "cand": cand, "candExcl": cm, "masks": masks}
+
+
+def domain_div(n: int, box) -> tuple[int, int]:
+    b = np.ascontiguousarray(box, np.float32)
+    x, y = C.c_int(), C.c_int()
+    _lib.call("bnb_domain_div", n, b.ctypes.data_as(C.c_void_p), C.byref(x), C.byref(y))
+    return x.value, y.value

@@ -1,0 +1,226 @@
+/*
+ * libbnb -- B200-native nonbonded direct space for BLaDE (C ABI).
+ *
+ * Replaces BLaDE's nonbonded direct-space path: the pair-force routine
+ * getforce_nbdirect (src/nbdirect/nbdirect.h:7) fed by the Domdec neighbour
+ * list (src/domdec/domdec.h:93-110) and scaled by the Msld lambda blocks
+ * (src/msld/msld.h:134-139).  Plain C types only: every array argument is a
+ * device pointer unless its comment says "host", streams are cudaStream_t
+ * passed as void*, and every function returns 0 or a BNB_ERR_* code.  No
+ * function exits, traps or prints.
+ *
+ * Units follow the caller (AKMA by default: A, kcal/mol).  "force" arrays hold
+ * dU/dx, the quantity BLaDE keeps in State::force_d.
+ */
+#ifndef BNB_H
+#define BNB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes ------------------------------------------------------ */
+#define BNB_OK 0
+#define BNB_ERR_ARG 1          /* bad argument (null, size, method)          */
+#define BNB_ERR_CUDA 2         /* a CUDA call failed                         */
+#define BNB_ERR_CAPACITY 3     /* list capacity exceeded and could not grow  */
+#define BNB_ERR_UNSUPPORTED 4  /* feature outside this build (see message)   */
+#define BNB_ERR_STATE 5        /* call order (e.g. compute before rebuild)   */
+#define BNB_ERR_DEVICE 6       /* device status word reports a failure       */
+
+/* ---- device status bits (bnb_status) ------------------------------------ */
+#define BNB_STATUS_BLOCK_OVERFLOW 1
+#define BNB_STATUS_TILE_OVERFLOW 2
+#define BNB_STATUS_MASK_OVERFLOW 4
+#define BNB_STATUS_WORK_OVERFLOW 8
+#define BNB_STATUS_NONFINITE 16
+
+/* Same layout as struct NbondPotential, src/system/potential.h:106-110. */
+typedef struct { int siteBlock; float q; int typeIdx; } bnb_nbond;
+/* Same layout as struct VdwPotential, src/system/potential.h:112-114. */
+typedef struct { float c12, c6; } bnb_vdw;
+/* Same layout as struct VariableBias, src/msld/msld.h:13-19. */
+typedef struct { int i, j, type; float l0, k; int n; } bnb_varbias;
+
+/*
+ * Run parameters of the path: Cutoffs{betaEwald,rCut,rSwitch}
+ * (src/run/run.h:16-20), elecMethod/vdwMethod (run.h:28-38), the MSLD
+ * soft-core flag (src/msld/msld.h:89) and the list pad
+ * (Domdec::cullPad, src/domdec/domdec.cu:138).
+ */
+typedef struct {
+  float rCut, rSwitch, betaEwald;
+  int elecMethod;        /* 0 FSWITCH, 1 PME, 2 FSHIFT */
+  int vdwMethod;         /* 0 VFSWITCH, 1 VSWITCH, 2 VSHIFT */
+  int useSoftCore;
+  float cullPad;         /* list buffer in length units (reference: computed) */
+  float kElectric;       /* 332.0716 AKMA, 138.935455103336 NMPS (defines.h) */
+  float softCoreRadius;  /* 4.0 AKMA, 0.4 NMPS (defines.h:48,74) */
+} bnb_params;
+
+/* Fills defaults: AKMA units, PME + VFSWITCH, rCut 12, rSwitch 10, beta 0.32,
+ * soft core on, pad 2. */
+void bnb_default_params(bnb_params *p);
+
+typedef struct bnb_handle bnb_handle;
+
+/*
+ * Creates a handle for `replicas` independent systems that share `p`.
+ * atomCounts: host [replicas].  Allocates device memory on the current device
+ * (the counterpart of Domdec::initialize, src/domdec/domdec.cu:83-199).
+ */
+int bnb_create(const bnb_params *p, int replicas, const int *atomCounts,
+               bnb_handle **out);
+int bnb_destroy(bnb_handle *h);
+
+/*
+ * Topology of all replicas, concatenated (host arrays):
+ *   nbonds[N]   per-atom {siteBlock,q,typeIdx}; siteBlock=(site<<16)|block
+ *               with blocks numbered within each replica (Msld::nbond_scaling,
+ *               src/msld/msld.cu:670-673); typeIdx indexes that replica's table.
+ *   typeCounts  host [replicas]; vdw: concatenated per-replica tables of
+ *               typeCounts[r]^2 entries (Potential::vdwParameters,
+ *               src/system/potential.cxx:1369-1403).
+ *   lambdaCounts host [replicas]: MSLD blocks per replica (1 = no alchemy).
+ *   excl[2*exclCount] directed atom pairs, atom indices local to their replica,
+ *               replica given by exclReplica[exclCount] (Potential::excls,
+ *               src/system/potential.cxx:1156-1163).  exclReplica may be NULL
+ *               when replicas==1.
+ */
+int bnb_set_topology(bnb_handle *h, const bnb_nbond *nbonds,
+                     const int *typeCounts, const bnb_vdw *vdw,
+                     const int *lambdaCounts, int exclCount, const int *excl,
+                     const int *exclReplica);
+
+/*
+ * Rebuilds the block list from coordinates (the counterpart of
+ * Domdec::reset_domdec, src/domdec/domdec.cu:201-211: bin, sort, 32-atom
+ * blocks, AABBs, half-shell cull at rCut+cullPad, exclusion masks).
+ * position: device float [3N] (State::position_fd layout, all replicas).
+ * boxes: host float [3*replicas] orthorhombic edges.
+ * flags: 0 = synchronise and grow capacities on overflow (as the reference's
+ * cull loop, src/domdec/cull.cu:337-375); BNB_ASYNC = enqueue only (graph
+ * capturable), overflow is reported through bnb_status and the pair kernel
+ * then does no work.
+ */
+#define BNB_ASYNC 1
+int bnb_rebuild(bnb_handle *h, const float *position, const float *boxes,
+                void *stream, int flags);
+
+/*
+ * One direct-space evaluation (getforce_nbdirect, src/nbdirect/nbdirect.cu:574;
+ * pack_positions + recull_blocks + kernel + unpack_forces, :492-526).
+ * position: device float [3N]; lambda: device float [sum lambdaCounts]
+ * (State::lambda_fd, ignored for replicas without alchemy); boxes host
+ * [3*replicas].  Outputs (device, any may be NULL):
+ *   force        float [3N]   dU/dx ADDED (State::force_d)
+ *   lambdaForce  float [sum lambdaCounts] dU/dlambda ADDED (State::lambdaForce_d)
+ *   energy       double [replicas] ADDED (State::energy_d[eenbdirect])
+ *   force64      double [3N]  OVERWRITTEN with the exact fixed-point totals
+ *   lambdaForce64 double [sum lambdaCounts] OVERWRITTEN
+ *   energy64     double [replicas] OVERWRITTEN
+ * calcEnergy selects the energy path as in the reference.
+ */
+typedef struct {
+  float *force;
+  float *lambdaForce;
+  double *energy;
+  double *force64;
+  double *lambdaForce64;
+  double *energy64;
+} bnb_outputs;
+int bnb_compute(bnb_handle *h, const float *position, const float *lambda,
+                const float *boxes, int calcEnergy, const bnb_outputs *out,
+                void *stream);
+
+/*
+ * Sets list capacities (candidate tiles, 32-row exclusion masks, work items)
+ * before the next rebuild; values <= 0 keep the current/estimated size.  The
+ * counterpart of the reference's maxPartnersPerBlock / maxBlockExclCount
+ * heuristics (src/domdec/domdec.cu:124-139).  A synchronous rebuild still
+ * grows any capacity that overflows; an asynchronous one reports the overflow.
+ */
+int bnb_reserve(bnb_handle *h, int tiles, int masks, int work);
+
+/* Device status word (ORed BNB_STATUS_* bits since the last clear);
+ * synchronises the stream.  clear!=0 resets it. */
+int bnb_status(bnb_handle *h, void *stream, int clear, int *status);
+
+/* Sizes of the current list (synchronises): blocks, candidate tiles, mask
+ * rows (in 32-row units), work items. */
+int bnb_list_sizes(bnb_handle *h, void *stream, int *blocks, int *tiles,
+                   int *masks, int *work);
+
+/*
+ * Copies the list structures to host arrays (test and inspection hook;
+ * synchronises).  Sizes from bnb_list_sizes.  Any pointer may be NULL.
+ *   wrap[N] blockBounds[B+1] sortedAtom[N] slotAtom[32B] bmin/bmax[3B]
+ *   candStart[B+1] cand[2*T] (jBlock, shiftCode) candMask[T] masks[32*M]
+ */
+int bnb_get_list(bnb_handle *h, void *stream, int *wrap, int *blockBounds,
+                 int *sortedAtom, int *slotAtom, float *bmin, float *bmax,
+                 int *candStart, int *cand, int *candMask, uint32_t *masks);
+
+/* Pairs with r<rCut evaluated by the last bnb_compute with counting enabled
+ * (bnb_set_counting).  Synchronises. */
+int bnb_set_counting(bnb_handle *h, int enable);
+int bnb_pair_count(bnb_handle *h, void *stream, unsigned long long *pairs);
+
+/*
+ * Per-phase timing with CUDA events recorded on the launching stream
+ * (profiling aid, no reference counterpart).  When enabled, every
+ * bnb_compute records events around the pair kernel and every bnb_rebuild
+ * around the list build.  bnb_profile_read synchronises, returns the summed
+ * milliseconds and counts since the last reset, and the number of kernels
+ * libbnb launched.
+ */
+int bnb_profile(bnb_handle *h, int enable);
+int bnb_profile_read(bnb_handle *h, double *pairMs, int *pairLaunches,
+                     double *rebuildMs, int *rebuilds,
+                     unsigned long long *kernelLaunches, int reset);
+
+/* Measured FP32 FMA throughput of the current device (flop/s), the roofline
+ * denominator of the FP32-bound pair kernel.  No reference counterpart. */
+int bnb_fp32_peak(void *stream, double *flopsPerSecond);
+
+/* Heuristic column grid of one replica (Domdec::initialize,
+ * src/domdec/domdec.cu:114-117), host computation. */
+int bnb_domain_div(int atomCount, const float *box, int *divX, int *divY);
+
+/* ---- MSLD lambda maps and biases (stateless, device arrays) -------------- */
+/*
+ * lambda_j = exp(fnex*sin(theta_j)) / sum over the site, FP64
+ * (Msld::calc_lambda_from_theta, src/msld/msld.cu:863-921).  Also writes the
+ * FP32 mirror lambda_f (State::lambda_fd) when non-NULL.  siteBound[sites+1],
+ * blockFixed[blocks] (may be NULL): fixed blocks keep lambda = theta.
+ */
+int bnb_lambda_from_theta(int siteCount, const int *siteBound, double fnex,
+                          const double *theta, const int *blockFixed,
+                          double *lambda, float *lambda_f, void *stream);
+/*
+ * dU/dtheta from dU/dlambda (Msld::calc_thetaForce_from_lambdaForce,
+ * src/msld/msld.cu:937-998).  thetaForce is ADDED to.
+ */
+int bnb_theta_force(int blockCount, const int *lambdaSite,
+                    const int *siteBound, double fnex, const double *lambda,
+                    const double *theta, const double *lambdaForce,
+                    const int *blockFixed, double *thetaForce, void *stream);
+/*
+ * Fixed bias b_i*lambda_i and variable biases (types 1-12) on lambda
+ * (Msld::getforce_fixedBias/getforce_variableBias, src/msld/msld.cu:1000-1153).
+ * lambdaForce and energy (may be NULL) are ADDED to.
+ */
+int bnb_bias(int blockCount, const double *lambda, const double *fixedBias,
+             int varCount, const bnb_varbias *varBias, double *lambdaForce,
+             double *energy, void *stream);
+
+/* Library version string. */
+const char *bnb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

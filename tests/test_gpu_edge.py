@@ -1,0 +1,148 @@
+"""GPU edge cases: capacity overflow and regrowth, asynchronous overflow
+reporting, non-finite input, tiny and uneven systems, MSLD lambda kernels."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from blade_b200 import msld as gmsld
+from blade_b200 import systems, _lib
+from blade_b200.nbdirect import NbDirect
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_rms(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
+
+
+def test_overflow_regrows_in_sync_rebuild(cuda):
+    """Undersized tile/mask/work capacities grow like cull.cu:337-375."""
+    s = systems.water_box()
+    nb = NbDirect(s)
+    nb.reserve(tiles=16, masks=2, work=4)
+    pos = nb.positions_tensor()
+    nb.update_domdec(pos, True)
+    assert nb.status() & 15 == 0
+    f, _, e = nb.evaluate(pos)
+    o = oracle.nbdirect(s)
+    assert rel_rms(f.cpu().numpy(), o["grad"]) <= 1e-5
+    nb.close()
+
+
+def test_async_overflow_is_reported_and_skipped(cuda):
+    s = systems.water_box()
+    nb = NbDirect(s)
+    nb.reserve(tiles=16, masks=2, work=4)
+    pos = nb.positions_tensor()
+    nb.update_domdec(pos, True, asynchronous=True)
+    st = nb.status()
+    assert st & _lib.STATUS_TILE_OVERFLOW
+    f, _, e = nb.evaluate(pos)           # pair kernel does no work on an invalid list
+    assert float(f.abs().sum()) == 0.0
+    nb.update_domdec(pos, True)          # a synchronous rebuild recovers
+    assert nb.status() & 15 == 0
+    f, _, _ = nb.evaluate(pos)
+    assert rel_rms(f.cpu().numpy(), oracle.nbdirect(s)["grad"]) <= 1e-5
+    nb.close()
+
+
+def test_nonfinite_coordinates_flagged(cuda):
+    s = systems.water_box()
+    s.xyz = s.xyz.copy()
+    s.xyz[5, 1] = np.nan
+    nb = NbDirect(s)
+    pos = nb.positions_tensor()
+    nb.update_domdec(pos, True)
+    nb.evaluate(pos)
+    assert nb.status() & _lib.STATUS_NONFINITE
+    nb.close()
+
+
+def test_small_and_sparse_systems(cuda):
+    # a handful of atoms in a big box: blocks with 1-3 atoms, many empty columns
+    rng = np.random.default_rng(3)
+    s = systems.water_box()
+    s.xyz = (rng.uniform(0, 30, (9, 3))).astype(np.float32)
+    s.box = np.float32([30, 30, 30])
+    s.nbonds = s.nbonds[:9].copy()
+    s.excl = s.excl[(s.excl < 9).all(1)]
+    nb = NbDirect(s)
+    pos = nb.positions_tensor()
+    nb.update_domdec(pos, True)
+    nb.set_counting(True)
+    f, _, e = nb.evaluate(pos)
+    o = oracle.nbdirect(s)
+    assert nb.pair_count() == o["pairs"]
+    assert rel_rms(f.cpu().numpy(), o["grad"]) <= 1e-5
+    nb.close()
+
+
+def test_atoms_on_box_faces(cuda):
+    s = systems.water_box()
+    s.xyz = s.xyz.copy()
+    L = float(s.box[0])
+    s.xyz[0] = [0.0, 0.0, 0.0]
+    s.xyz[3] = [L, L * 0.5, np.nextafter(np.float32(L), np.float32(0))]
+    s.xyz[6] = [-0.0, L, 1e-7]
+    nb = NbDirect(s)
+    pos = nb.positions_tensor()
+    nb.update_domdec(pos, True)
+    g = nb.get_list()
+    o = oracle.build_list(s)
+    for k in ("wrap", "sortedAtom", "cand", "masks"):
+        assert np.array_equal(g[k], o[k]), k
+    nb.close()
+
+
+def test_list_reuse_between_rebuilds(cuda):
+    """Positions move between rebuilds; the pad keeps every pair (Domdec freqDomdec)."""
+    s = systems.water_box()
+    rng = np.random.default_rng(9)
+    nb = NbDirect(s)
+    nb.update_domdec(nb.positions_tensor(), True)
+    x = s.xyz.copy()
+    for _ in range(5):
+        x = (x + rng.normal(0, 0.08, x.shape)).astype(np.float32)
+        pos = nb.positions_tensor([x])
+        nb.set_counting(True)
+        f, _, _ = nb.evaluate(pos)
+        o = oracle.nbdirect(s, xyz=x)
+        assert nb.pair_count() == o["pairs"]
+        assert rel_rms(f.cpu().numpy(), o["grad"]) <= 1e-5
+    nb.close()
+
+
+def test_msld_lambda_kernels(cuda):
+    bound = np.array([0, 1, 4, 8, 11], np.int32)
+    site = np.array([0, 1, 1, 1, 2, 2, 2, 2, 3, 3, 3], np.int32)
+    rng = np.random.default_rng(2)
+    th = rng.uniform(-2, 2, 11)
+    th[0] = 1.0
+    fixed = np.zeros(11, np.int32)
+    fixed[0] = 1
+    dev = lambda a: torch.from_numpy(a).cuda()
+    lam = torch.zeros(11, dtype=torch.float64, device="cuda")
+    lamf = torch.zeros(11, dtype=torch.float32, device="cuda")
+    gmsld.lambda_from_theta(dev(bound), 5.5, dev(th), lam, lamf, dev(fixed))
+    ol = oracle.lambda_from_theta(bound, 5.5, th, fixed)
+    np.testing.assert_allclose(lam.cpu().numpy(), ol, rtol=1e-13, atol=1e-15)
+    F = rng.normal(size=11)
+    tf = torch.zeros(11, dtype=torch.float64, device="cuda")
+    gmsld.theta_force(dev(site), dev(bound), 5.5, lam, dev(th), dev(F), tf, dev(fixed))
+    np.testing.assert_allclose(tf.cpu().numpy(), oracle.theta_force(site, bound, 5.5, ol, th, F, fixed),
+                               rtol=1e-12, atol=1e-12)
+    vb = np.zeros(4, gmsld.VARBIAS_DTYPE)
+    vb[0] = (1, 2, 6, 0.0, 2.0, 0)
+    vb[1] = (1, 3, 8, 0.017, -1.5, 0)
+    vb[2] = (4, 5, 10, -5.56, 0.7, 0)
+    vb[3] = (5, 9, 6, 0.0, 3.0, 0)
+    fb = rng.normal(size=11)
+    lf = torch.zeros(11, dtype=torch.float64, device="cuda")
+    en = torch.zeros(1, dtype=torch.float64, device="cuda")
+    vbd = torch.from_numpy(vb.view(np.uint8).copy()).cuda()
+    gmsld.bias(lam, dev(fb), vbd, lf, en)
+    olf, oe = oracle.bias(ol, fb, vb)
+    np.testing.assert_allclose(lf.cpu().numpy(), olf, rtol=1e-5, atol=1e-6)
+    assert float(en[0]) == pytest.approx(oe, rel=1e-6)
