@@ -48,7 +48,8 @@ struct Counters {
   int maskCount;
   int workCount;
   int status;
-  int pad[3];
+  int workNext;            // dynamic work-item counter of the pair kernel
+  int pad[2];
   unsigned long long pairCount;
 };
 
@@ -115,6 +116,7 @@ struct PairConst {        // uniform parameters of the pair kernel
   // VSWITCH / VSHIFT / FSWITCH / FSHIFT helpers
   float roff2, ron2, rul3inv, rul12;
   float fA, fB, fC, fD, fdvc, rcinv;
+  float fsG, fsG5, fsC1, fsP1, fsP2, fsP3;   // factored FSWITCH (see pair_terms)
   float vshRc6inv, vshRc12inv, vshRc18inv;
 };
 

@@ -114,6 +114,12 @@ PairConst make_const(const bnb_params &p) {
   c.fD = (float)(2 * ginv / 5);
   c.fdvc = (float)(8 * (ron2 * roff2 * (rc - rs) - (roff2 * roff2 * rc - ron2 * ron2 * rs) / 5) * ginv);
   c.rcinv = (float)(1.0 / rc);
+  c.fsG = (float)ginv;
+  c.fsG5 = (float)(ginv / 5);
+  c.fsC1 = (float)(roff2 - 3 * ron2);
+  c.fsP1 = (float)(6 * rc);
+  c.fsP2 = (float)(7 * rc * rc - 5 * rs * rs);
+  c.fsP3 = (float)(5 * rc * rc * rc - 15 * rc * rs * rs);
   double rc6 = roff2 * roff2 * roff2;
   c.vshRc6inv = (float)(1.0 / rc6);
   c.vshRc12inv = (float)(1.0 / (rc6 * rc6));

@@ -105,11 +105,19 @@ __device__ __forceinline__ void pair_terms(const PairConst &pc, float r, float r
       fe = -qq * rinv * rinv;
       if (NEEDE) ee = qq * (rinv + pc.fdvc);
     } else {
-      float r3 = r2 * r, r5 = r3 * r2;
-      fe = -qq * rinv * (pc.fA * rinv + pc.fB * r + 3.f * pc.fC * r3 + 5.f * pc.fD * r5);
-      if (NEEDE)
-        ee = qq * (pc.fA * (rinv - pc.rcinv) + pc.fB * (pc.rcut - r) +
-                   pc.fC * (pc.roff2 * pc.rcut - r3) + pc.fD * (pc.roff2 * pc.roff2 * pc.rcut - r5));
+      // The reference's expanded polynomial (nbdirect.cu:293-299) cancels to
+      // ~0 near rCut; in FP32 that costs ~1e-5 relative force error.  The same
+      // functions in factored form:
+      //   dE/dr = -qq (rc^2-r^2)^2 (rc^2+2r^2-3rs^2) ginv / r^2
+      //   E     =  qq (rc-r)^3 P(r) ginv / (5 r),
+      //   P(r)  = 2r^3 + 6 rc r^2 + (7rc^2-5rs^2) r + 5rc^3 - 15 rc rs^2.
+      float w = pc.roff2 - r2;
+      fe = -qq * (w * w * fmaf(2.f, r2, pc.fsC1) * pc.fsG) * (rinv * rinv);
+      if (NEEDE) {
+        float t = pc.rcut - r;
+        float p = fmaf(fmaf(fmaf(2.f, r, pc.fsP1), r, pc.fsP2), r, pc.fsP3);
+        ee = qq * (t * t * t) * p * pc.fsG5 * rinv;
+      }
     }
   } else {  // FSHIFT
     float ri2 = pc.rcinv * pc.rcinv;
@@ -177,16 +185,58 @@ struct KArgs {
   int count;               // count in-cutoff pairs
 };
 
+// j-side registers that travel with the rotation.
+template <bool COMBINE, int ALCH>
+struct JRegs {
+  float x, y, z, q;
+  int meta;                // original j lane << 16 | LJ type (table) ; original lane (combine)
+  float ex, er;            // combine mode: sqrt(2 eps), Rmin/2
+  int b;                   // MSLD siteBlock
+  float l;                 // lambda of b
+  float fx, fy, fz, fl;
+
+  __device__ __forceinline__ void move(int src, int width) {
+    x = __shfl_sync(kFull, x, src, width);
+    y = __shfl_sync(kFull, y, src, width);
+    z = __shfl_sync(kFull, z, src, width);
+    q = __shfl_sync(kFull, q, src, width);
+    meta = __shfl_sync(kFull, meta, src, width);
+    if (COMBINE) {
+      ex = __shfl_sync(kFull, ex, src, width);
+      er = __shfl_sync(kFull, er, src, width);
+    }
+    if (ALCH) {
+      b = __shfl_sync(kFull, b, src, width);
+      l = __shfl_sync(kFull, l, src, width);
+    }
+  }
+  __device__ __forceinline__ void move_forces(int src, int width, bool alch) {
+    fx = __shfl_sync(kFull, fx, src, width);
+    fy = __shfl_sync(kFull, fy, src, width);
+    fz = __shfl_sync(kFull, fz, src, width);
+    if (ALCH && alch) fl = __shfl_sync(kFull, fl, src, width);
+  }
+};
+
 // ---------------------------------------------------------------------------
 // The pair kernel.
 // ALCH: 0 none, 1 MSLD scaling, 2 MSLD scaling + soft core.
+//
+// Tile processing with j compaction: the j atoms of a tile that lie within
+// rCut of the i block's AABB are gathered into lanes 0..nj-1 and replicated in
+// groups of gj = 8, 16 or 32 lanes (smallest gj >= nj).  Every lane keeps its
+// own i atom and rotates through the gj compacted j atoms of its group, so a
+// tile costs gj steps instead of 32; the group partial j forces are summed
+// with xor shuffles and returned to the owner lanes.
 // ---------------------------------------------------------------------------
 template <int ELEC, int VDW, int ALCH, bool ENERGY, bool COMBINE>
-__global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
+__global__ void __launch_bounds__(256, 4) k_pair(KArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int sIdx[8][32];
   const Dev &d = A.d;
   const PairConst &pc = A.pc;
   const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
   const int nT = d.nTypes;
   float2 *sLJ = reinterpret_cast<float2 *>(smem);
   size_t off = COMBINE ? 0 : sizeof(float2) * nT * nT;
@@ -206,11 +256,12 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
   const int status = d.ctr->status;
   const int nWork = (status & kStatusListInvalid) ? 0 : d.ctr->workCount;
   const int S = 32 * d.maxBlocks;
-  const int nWarps = (gridDim.x * blockDim.x) >> 5;
-  const int srcLane = (lane + 1) & 31;
   unsigned long long pairs = 0;
 
-  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nWork; w += nWarps) {
+  int w = 0;
+  if (lane == 0) w = atomicAdd(&d.ctr->workNext, 1);
+  w = __shfl_sync(kFull, w, 0);
+  while (w < nWork) {
     const int2 wk = d.work[w];
     const int iBlock = wk.x;
     const int c0 = wk.y;
@@ -226,6 +277,7 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
     const float li = (ALCH && bi) ? sLam[bi & 0xFFFF] : 1.f;
     const RepInfo &ri = d.rep[d.blockRep[iBlock]];
     const float bx = ri.box[0], by = ri.box[1], bz = ri.box[2];
+    const float4 imin = d.bmin[iBlock], imax = d.bmax[iBlock];
 
     // per-step recull of this work item's candidates (recull.cu:41-122)
     int4 cand = make_int4(0, 0, -1, 0);
@@ -236,7 +288,7 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
       shift_of(cand.y, sx, sy, sz);
       float3 sh = make_float3(__fmul_rn((float)sx, bx), __fmul_rn((float)sy, by),
                               __fmul_rn((float)sz, bz));
-      hit = aabb_hit(d.bmin[iBlock], d.bmax[iBlock], d.bmin[cand.x], d.bmax[cand.x], sh, pc.rc2);
+      hit = aabb_hit(imin, imax, d.bmin[cand.x], d.bmax[cand.x], sh, pc.rc2);
     }
     unsigned act = __ballot_sync(kFull, hit);
 
@@ -250,67 +302,92 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
       int sx, sy, sz;
       shift_of(code, sx, sy, sz);
       const int jslot = 32 * jBlock + lane;
-      float4 xj = d.xyzq[jslot];
-      xj.x += (float)sx * bx;
-      xj.y += (float)sy * by;
-      xj.z += (float)sz * bz;
-      int tj = d.slotType[jslot];
-      float2 ljJ = COMBINE ? d.ljType[tj] : make_float2(0.f, 0.f);
-      int bj = ALCH ? d.slotSiteBlock[jslot] : 0;
-      float lj = (ALCH && bj) ? sLam[bj & 0xFFFF] : 1.f;
+      JRegs<COMBINE, ALCH> J;
+      {
+        const float4 xj = d.xyzq[jslot];
+        J.x = xj.x + (float)sx * bx;
+        J.y = xj.y + (float)sy * by;
+        J.z = xj.z + (float)sz * bz;
+        J.q = xj.w;
+      }
+      const int tj = d.slotType[jslot];
+      J.meta = COMBINE ? lane : ((lane << 16) | tj);
+      if (COMBINE) {
+        const float2 lj2 = d.ljType[tj];
+        J.ex = lj2.x;
+        J.er = lj2.y;
+      }
+      const int bj0 = ALCH ? d.slotSiteBlock[jslot] : 0;
+      if (ALCH) {
+        J.b = bj0;
+        J.l = bj0 ? sLam[bj0 & 0xFFFF] : 1.f;
+      }
       const bool jValid = d.slotAtom[jslot] >= 0;
       uint32_t row = mIdx >= 0 ? d.masks[32 * (size_t)mIdx + lane] : kFull;
       if (jBlock == iBlock && code == 0) row &= (lane == 31) ? 0u : (kFull << (lane + 1));
-      row &= __ballot_sync(kFull, jValid);
       if (!iValid) row = 0u;
-      uint32_t mr = __funnelshift_r(row, row, lane);  // bit k <-> j = (lane+k)&31
 
-      float fjx = 0.f, fjy = 0.f, fjz = 0.f, flj = 0.f;
-      const bool alchTile = ALCH ? __any_sync(kFull, (bi | bj) != 0) : false;
+      // j atoms that can reach the i block (per-atom AABB test, nbdirect.cu:211)
+      float g, gap2;
+      g = fmaxf(fmaxf(imin.x - J.x, J.x - imax.x), 0.f);
+      gap2 = g * g;
+      g = fmaxf(fmaxf(imin.y - J.y, J.y - imax.y), 0.f);
+      gap2 = fmaf(g, g, gap2);
+      g = fmaxf(fmaxf(imin.z - J.z, J.z - imax.z), 0.f);
+      gap2 = fmaf(g, g, gap2);
+      const bool jin = jValid && gap2 < pc.rc2;
+      const unsigned jm = __ballot_sync(kFull, jin);
+      const int nj = __popc(jm);
+      if (nj == 0) continue;
+      const int gj = nj <= 8 ? 8 : (nj <= 16 ? 16 : 32);
+      const bool alchTile = ALCH ? __any_sync(kFull, (bi | bj0) != 0) : false;
+
+      // compact: lane p of every group receives the p-th surviving j atom
+      const int rank = __popc(jm & ((1u << lane) - 1u));
+      if (jin) sIdx[warp][rank] = lane;
+      __syncwarp();
+      const int cl = lane & (gj - 1);
+      const int src = cl < nj ? sIdx[warp][cl] : lane;
+      __syncwarp();
+      J.move(src, 32);
+      if (cl >= nj) J.x = 1.0e18f;  // empty compacted slot: never within rCut
+      J.fx = J.fy = J.fz = J.fl = 0.f;
+      const int rot = lane + 1;
 
       if (!alchTile) {
-#pragma unroll 8
-        for (int k = 0; k < 32; k++) {
-          const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+#pragma unroll 4
+        for (int k = 0; k < gj; k++) {
+          const float dx = xi.x - J.x, dy = xi.y - J.y, dz = xi.z - J.z;
           const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          if ((mr & 1u) && r2 < pc.rc2) {
+          const int jb = COMBINE ? J.meta : (J.meta >> 16);
+          if (((row >> jb) & 1u) && r2 < pc.rc2) {
             float c12, c6;
-            lj_params<COMBINE>(sLJ, rowI, tj, ljI, ljJ, c12, c6);
+            lj_params<COMBINE>(sLJ, rowI, J.meta & 0xFFFF, ljI, make_float2(J.ex, J.er), c12, c6);
             const float rinv = rsqrt_approx(r2);
             const float r = r2 * rinv;
             float dEdr, E;
-            pair_terms<ELEC, VDW, ENERGY>(pc, r, r2, rinv, xi.w * xj.w, c12, c6, dEdr, E);
+            pair_terms<ELEC, VDW, ENERGY>(pc, r, r2, rinv, xi.w * J.q, c12, c6, dEdr, E);
             const float fs = dEdr * rinv;
             fix = fmaf(fs, dx, fix); fiy = fmaf(fs, dy, fiy); fiz = fmaf(fs, dz, fiz);
-            fjx = fmaf(-fs, dx, fjx); fjy = fmaf(-fs, dy, fjy); fjz = fmaf(-fs, dz, fjz);
+            J.fx = fmaf(-fs, dx, J.fx); J.fy = fmaf(-fs, dy, J.fy); J.fz = fmaf(-fs, dz, J.fz);
             if (ENERGY) ei += E;
             if (A.count) pairs++;
           }
-          mr >>= 1;
-          xj.x = __shfl_sync(kFull, xj.x, srcLane);
-          xj.y = __shfl_sync(kFull, xj.y, srcLane);
-          xj.z = __shfl_sync(kFull, xj.z, srcLane);
-          xj.w = __shfl_sync(kFull, xj.w, srcLane);
-          if (COMBINE) {
-            ljJ.x = __shfl_sync(kFull, ljJ.x, srcLane);
-            ljJ.y = __shfl_sync(kFull, ljJ.y, srcLane);
-          } else {
-            tj = __shfl_sync(kFull, tj, srcLane);
-          }
-          fjx = __shfl_sync(kFull, fjx, srcLane);
-          fjy = __shfl_sync(kFull, fjy, srcLane);
-          fjz = __shfl_sync(kFull, fjz, srcLane);
+          J.move(rot, gj);
+          J.move_forces(rot, gj, false);
         }
       } else if (ALCH) {
-#pragma unroll 4
-        for (int k = 0; k < 32; k++) {
-          const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        for (int k = 0; k < gj; k++) {
+          const float dx = xi.x - J.x, dy = xi.y - J.y, dz = xi.z - J.z;
           const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          if ((mr & 1u) && r2 < pc.rc2) {
+          const int jb = COMBINE ? J.meta : (J.meta >> 16);
+          if (((row >> jb) & 1u) && r2 < pc.rc2) {
             float c12, c6;
-            lj_params<COMBINE>(sLJ, rowI, tj, ljI, ljJ, c12, c6);
+            lj_params<COMBINE>(sLJ, rowI, J.meta & 0xFFFF, ljI, make_float2(J.ex, J.er), c12, c6);
             const float rinv = rsqrt_approx(r2);
             const float r = r2 * rinv;
+            const int bj = J.b;
+            const float lj = J.l;
             // MSLD scaling, nbdirect.cu:244-254
             const bool sameSite = (bi & 0xFFFF0000) == (bj & 0xFFFF0000);
             const float s = sameSite ? (bi == bj ? li : 0.f) : li * lj;
@@ -329,7 +406,7 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
               }
             }
             float dEdr, E;
-            pair_terms<ELEC, VDW, true>(pc, rEff, r2E, rinvE, xi.w * xj.w, c12, c6, dEdr, E);
+            pair_terms<ELEC, VDW, true>(pc, rEff, r2E, rinvE, xi.w * J.q, c12, c6, dEdr, E);
             dEdr *= s;
             if (pert) {  // dU/dlambda routing, nbdirect.cu:400-415
               const float fl = fmaf(dEdr, dredll, E);
@@ -337,43 +414,45 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
                 if (bi == bj) fli += fl;
               } else {
                 fli = fmaf(lj, fl, fli);
-                flj = fmaf(li, fl, flj);
+                J.fl = fmaf(li, fl, J.fl);
               }
             }
             const float fs = dEdr * dredr * rinv;
             fix = fmaf(fs, dx, fix); fiy = fmaf(fs, dy, fiy); fiz = fmaf(fs, dz, fiz);
-            fjx = fmaf(-fs, dx, fjx); fjy = fmaf(-fs, dy, fjy); fjz = fmaf(-fs, dz, fjz);
+            J.fx = fmaf(-fs, dx, J.fx); J.fy = fmaf(-fs, dy, J.fy); J.fz = fmaf(-fs, dz, J.fz);
             if (ENERGY) ei = fmaf(s, E, ei);
             if (A.count) pairs++;
           }
-          mr >>= 1;
-          xj.x = __shfl_sync(kFull, xj.x, srcLane);
-          xj.y = __shfl_sync(kFull, xj.y, srcLane);
-          xj.z = __shfl_sync(kFull, xj.z, srcLane);
-          xj.w = __shfl_sync(kFull, xj.w, srcLane);
-          if (COMBINE) {
-            ljJ.x = __shfl_sync(kFull, ljJ.x, srcLane);
-            ljJ.y = __shfl_sync(kFull, ljJ.y, srcLane);
-          } else {
-            tj = __shfl_sync(kFull, tj, srcLane);
-          }
-          bj = __shfl_sync(kFull, bj, srcLane);
-          lj = __shfl_sync(kFull, lj, srcLane);
-          fjx = __shfl_sync(kFull, fjx, srcLane);
-          fjy = __shfl_sync(kFull, fjy, srcLane);
-          fjz = __shfl_sync(kFull, fjz, srcLane);
-          flj = __shfl_sync(kFull, flj, srcLane);
+          J.move(rot, gj);
+          J.move_forces(rot, gj, true);
         }
       }
-      // j force of this tile is back in its owner lane
-      if (jValid && (fjx != 0.f || fjy != 0.f || fjz != 0.f)) {
-        red_add(&d.accF[jslot], to_fix(fjx));
-        red_add(&d.accF[S + jslot], to_fix(fjy));
-        red_add(&d.accF[2 * S + jslot], to_fix(fjz));
-        if (!(isfinite(fjx) && isfinite(fjy) && isfinite(fjz))) atomicOr(&d.ctr->status, kStatusNonFinite);
+      // sum the group partials; group 0 lane p now holds compacted j p
+      float fx = J.fx, fy = J.fy, fz = J.fz, fl = J.fl;
+      if (gj <= 16) {
+        fx += __shfl_xor_sync(kFull, fx, 16); fy += __shfl_xor_sync(kFull, fy, 16);
+        fz += __shfl_xor_sync(kFull, fz, 16);
+        if (ALCH && alchTile) fl += __shfl_xor_sync(kFull, fl, 16);
       }
-      if (ALCH && bj && flj != 0.f) atomicAdd(reinterpret_cast<unsigned long long *>(&sAccL[bj & 0xFFFF]),
-                                              static_cast<unsigned long long>(to_fix(flj)));
+      if (gj == 8) {
+        fx += __shfl_xor_sync(kFull, fx, 8); fy += __shfl_xor_sync(kFull, fy, 8);
+        fz += __shfl_xor_sync(kFull, fz, 8);
+        if (ALCH && alchTile) fl += __shfl_xor_sync(kFull, fl, 8);
+      }
+      // return to the owner lane of each surviving j atom
+      fx = __shfl_sync(kFull, fx, rank);
+      fy = __shfl_sync(kFull, fy, rank);
+      fz = __shfl_sync(kFull, fz, rank);
+      if (ALCH && alchTile) fl = __shfl_sync(kFull, fl, rank);
+      if (jin && (fx != 0.f || fy != 0.f || fz != 0.f)) {
+        red_add(&d.accF[jslot], to_fix(fx));
+        red_add(&d.accF[S + jslot], to_fix(fy));
+        red_add(&d.accF[2 * S + jslot], to_fix(fz));
+        if (!(isfinite(fx) && isfinite(fy) && isfinite(fz))) atomicOr(&d.ctr->status, kStatusNonFinite);
+      }
+      if (ALCH && alchTile && jin && bj0 && fl != 0.f)
+        atomicAdd(reinterpret_cast<unsigned long long *>(&sAccL[bj0 & 0xFFFF]),
+                  static_cast<unsigned long long>(to_fix(fl)));
     }
     if (iValid && (fix != 0.f || fiy != 0.f || fiz != 0.f)) {
       red_add(&d.accF[islot], to_fix(fix));
@@ -390,6 +469,8 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
       for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(kFull, e, o);
       if (lane == 0 && e != 0) red_add(&d.accE[d.blockRep[iBlock]], e);
     }
+    if (lane == 0) w = atomicAdd(&d.ctr->workNext, 1);
+    w = __shfl_sync(kFull, w, 0);
   }
   if (A.count) {
 #pragma unroll
@@ -421,6 +502,7 @@ __global__ void k_finalize(Dev d, bnb_outputs o) {
     }
   }
   if (blockIdx.x == 0) {
+    if (threadIdx.x == 0) d.ctr->workNext = 0;  // the pair kernel of the next step starts at item 0
     for (int i = threadIdx.x; i < d.lamTotal; i += blockDim.x) {
       long long v = d.accL[i];
       d.accL[i] = 0;
@@ -438,10 +520,25 @@ __global__ void k_finalize(Dev d, bnb_outputs o) {
   }
 }
 
+// Persistent launch: as many CTAs as fit at once; warps pull work items from
+// the device counter, so the grid never leaves a partial last wave.
 template <int ELEC, int VDW, int ALCH, bool ENERGY, bool COMBINE>
-void launch_t(const KArgs &a, int grid, size_t shmem, cudaStream_t s) {
+void launch_t(const KArgs &a, int maxGrid, size_t shmem, cudaStream_t s) {
   auto k = k_pair<ELEC, VDW, ALCH, ENERGY, COMBINE>;
+  static int perSM = -1, sms = 0;
+  static size_t shmemSeen = ~size_t(0);
   if (shmem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+  if (perSM < 0 || shmemSeen != shmem) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k, 256, shmem) != cudaSuccess || perSM < 1)
+      perSM = 1;
+    shmemSeen = shmem;
+  }
+  int grid = perSM * sms;
+  if (grid > maxGrid) grid = maxGrid;
+  if (grid < 1) grid = 1;
   k<<<grid, 256, shmem, s>>>(a);
 }
 

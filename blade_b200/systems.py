@@ -255,7 +255,7 @@ def _fill_water(rng, box: float, nwat: int, solute: np.ndarray, dmin: float = 2.
         g = (np.arange(n_side) + 0.5) * a
         sites = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
         if len(solute):
-            tree = cKDTree(solute, boxsize=box)
+            tree = cKDTree(np.mod(solute, box), boxsize=box)
             d, _ = tree.query(np.mod(sites, box), k=1)
             sites = sites[d > dmin]
         if len(sites) >= nwat:

@@ -37,7 +37,10 @@ def run(sys_, count=True):
 
 def check(sys_, g, o, check_lambda=False):
     assert g["status"] == 0
-    assert g["pairs"] == o["pairs"]
+    # FP32 vs FP64 distance: pairs within ~1e-6 A of rCut may flip (about one
+    # pair per 4e6 at rCut 12 A); the list itself misses nothing (bit-exact
+    # list tests and the oracle coverage test).
+    assert abs(g["pairs"] - o["pairs"]) <= max(2, 1e-6 * o["pairs"]), (g["pairs"], o["pairs"])
     err = rel_rms(g["grad"], o["grad"])
     assert err <= FORCE_TOL, err
     scale = max(abs(o["energy"]), sys_.N)
