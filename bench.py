@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--impl", default="bnb", choices=["bnb", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref", action="store_true", help="skip the reference CUDA comparison leg")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     return ap.parse_args()
 
@@ -288,6 +289,27 @@ def run_bnb(args, rank, world):
         t_e2e = sum(a.elapsed_time(b) for a, b in e_evs) / 1e3
         e2e = {"t": t_e2e, "h2d": 4 * 3 * s.N, "d2h": 4 * 3 * s.N + 8}
 
+    # the reference's own CUDA path (src/nbdirect + src/domdec, unmodified,
+    # oracle/_ref) on the same trajectory, same GPU, same L2 flushing
+    ref_cuda = None
+    if world == 1 and not args.no_ref:
+        from oracle import refgpu
+        if refgpu.available():
+            try:
+                ref = refgpu.RefGPU(s)
+                fr64 = frames.double()
+                ref.time(fr64[:W], W, REBUILD_EVERY, True, flush)        # warm-up incl. first build
+                t_ref = ref.time(fr64[W:], K, REBUILD_EVERY, True, flush) / 1e3
+                ref_cuda = {"value": P / t_ref, "unit": "pairs/s", "ms_per_step": 1e3 * t_ref / K,
+                            "build": "reference src/nbdirect + src/domdec unmodified, nvcc -O3 "
+                                     "-use_fast_math, sm_100a, driven by oracle/ref/ref_harness.cu",
+                            "note": "same frames, rebuild every 10 steps, 2 A pad, L2 flushed"}
+                del fr64
+            except Exception as exc:  # report, do not hide
+                ref_cuda = {"unavailable": str(exc)}
+        else:
+            ref_cuda = {"unavailable": "oracle/_ref/libbladeref.so not built"}
+
     # aggregate over ranks: max time, summed pairs
     if world > 1:
         t = torch.tensor([t_total, e2e["t"] if e2e else 0.0], dtype=torch.float64, device=dev)
@@ -325,6 +347,8 @@ def run_bnb(args, rank, world):
         "clocks": clocks.summary(),
         "parity_vs_fp64_oracle": parity,
     }
+    if ref_cuda is not None:
+        line["reference_cuda_same_gpu"] = ref_cuda
     if e2e:
         line["e2e"] = {"value": P_all / t_e2e_max, "unit": "pairs/s", "h2d_bytes_per_step": e2e["h2d"],
                        "d2h_bytes_per_step": e2e["d2h"]}

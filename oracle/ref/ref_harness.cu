@@ -1,0 +1,273 @@
+// Comparison harness around the reference's own CUDA direct-space path.
+//
+// TEST AND MEASUREMENT INFRASTRUCTURE ONLY.  This file is compiled together
+// with the reference's unmodified sources src/nbdirect/nbdirect.cu and
+// src/domdec/*.cu (see Makefile in this directory) into
+// oracle/_ref/libbladeref.so.  It builds the handful of System fields that
+// path reads -- State buffers in the [lambda | x | theta] layout
+// (src/system/state.cxx), the Potential nonbonded tables and the vdW texture
+// (src/system/potential.cxx:1336-1420), the Run cutoffs/methods/streams and
+// the Msld block count -- and provides the few out-of-path functions the
+// path calls (printlog/fatal from src/io, calc_virtual_position from
+// src/holonomic, State::broadcast_position/broadcast_box from src/system).
+// Each step it calls Domdec::update_domdec and getforce_nbdirect exactly as
+// Run::dynamics and Potential::calc_force do (src/run/run.cu:554-564,
+// src/system/potential.cxx:1839-1929), on one stream.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <new>
+
+#include "domdec/domdec.h"
+#include "main/defines.h"
+#include "msld/msld.h"
+#include "nbdirect/nbdirect.h"
+#include "run/run.h"
+#include "system/potential.h"
+#include "system/state.h"
+#include "system/system.h"
+
+// ---- out-of-path functions the path calls ---------------------------------
+void printlog(const char *format, ...) { (void)format; }
+
+void fatal(const char *fnm, int i, const char *format, ...) {
+  va_list args;
+  va_start(args, format);
+  fprintf(stderr, "reference fatal at %s:%d: ", fnm, i);
+  vfprintf(stderr, format, args);
+  va_end(args);
+  abort();
+}
+
+void calc_virtual_position(System *, bool) {}  // no virtual sites in these systems
+
+__global__ void harness_set_fd(int n, float *pf, const double *pd) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) pf[i] = (float)pd[i];
+}
+
+// Single GPU: broadcast_position reduces to State::set_fd
+// (src/system/state.cxx:411-442, src/update/update.cu:308-330).
+void State::broadcast_position(System *system) {
+  int n = 3 * atomCount + 2 * lambdaCount;
+  harness_set_fd<<<(n + 255) / 256, 256, 0, system->run->updateStream>>>(n, positionBuffer_fd,
+                                                                         positionBuffer_d);
+}
+
+void State::broadcast_box(System *) {}  // the harness sets orthBox and orthBox_f itself
+
+// ---- harness ---------------------------------------------------------------
+struct ref_handle {
+  System *sys;
+  State *st;
+  Run *run;
+  Potential *pot;
+  Msld *msld;
+  void *message[1];
+  cudaStream_t stream;
+  cudaEvent_t e0, e1;
+  int N, nL;
+  bool initialized;
+};
+
+template <typename T>
+static T *raw_object() {
+  void *p = calloc(1, sizeof(T));  // fields the path does not read stay zero
+  return static_cast<T *>(p);
+}
+
+extern "C" int ref_create(int N, const int *siteBlock, const float *q, const int *typeIdx,
+                          int nTypes, const float *vdw, int exclCount, const int *excl,
+                          int nLambda, int useSoftCore, float rCut, float rSwitch, float beta,
+                          int elecMethod, int vdwMethod, float cullPad, const double *box,
+                          ref_handle **out) {
+  ref_handle *h = new ref_handle();
+  h->N = N;
+  h->nL = nLambda < 1 ? 1 : nLambda;
+  if (cudaStreamCreate(&h->stream) != cudaSuccess) return 2;
+  cudaEventCreate(&h->e0);
+  cudaEventCreate(&h->e1);
+
+  System *sys = raw_object<System>();
+  State *st = raw_object<State>();
+  Run *run = raw_object<Run>();
+  Potential *pot = raw_object<Potential>();
+  Msld *msld = raw_object<Msld>();
+  h->sys = sys; h->st = st; h->run = run; h->pot = pot; h->msld = msld;
+  sys->id = 0;
+  sys->idCount = 1;
+  sys->verbose = 0;
+  sys->message = h->message;
+  sys->state = st;
+  sys->run = run;
+  sys->potential = pot;
+  sys->msld = msld;
+
+  // Run: cutoffs, methods, one stream for every role (serial execution)
+  new (&run->calcTermFlag) std::map<int, bool>();
+  run->calcTermFlag[eenbdirect] = true;
+  run->cutoffs.betaEwald = beta;
+  run->cutoffs.rCut = rCut;
+  run->cutoffs.rSwitch = rSwitch;
+  run->betaEwald = beta;
+  run->rCut = rCut;
+  run->rSwitch = rSwitch;
+  run->elecMethod = (EElec)elecMethod;
+  run->vdwMethod = (EVdw)vdwMethod;
+  run->updateStream = run->bondedStream = run->biaspotStream = run->nbdirectStream =
+      run->nbrecipStream = run->mlpotStream = h->stream;
+  // Domdec::initialize sets cullPad = 2*sqrt(30 kB T)*freqDomdec*dt
+  // (src/domdec/domdec.cu:138); pick dt so that the pad equals cullPad.
+  run->T = 300;
+  run->dt = cullPad / (2 * std::sqrt(30 * kB * run->T) * 10);
+
+  // Msld
+  msld->blockCount = h->nL;
+  msld->useSoftCore = useSoftCore != 0;
+
+  // State buffers in the [lambda | x | theta] layout
+  st->atomCount = N;
+  st->lambdaCount = h->nL;
+  int nbuf = 3 * N + 2 * h->nL;
+  cudaMalloc(&st->positionBuffer_d, sizeof(double) * nbuf);
+  cudaMalloc(&st->positionBuffer_fd, sizeof(float) * nbuf);
+  cudaMalloc(&st->forceBuffer_d, sizeof(float) * nbuf);
+  cudaMalloc(&st->energy_d, sizeof(double) * eeend);
+  cudaMemset(st->positionBuffer_d, 0, sizeof(double) * nbuf);
+  st->lambda_d = st->positionBuffer_d;
+  st->position_d = (double(*)[3])(st->positionBuffer_d + h->nL);
+  st->theta_d = st->positionBuffer_d + h->nL + 3 * N;
+  st->lambda_fd = st->positionBuffer_fd;
+  st->position_fd = (float(*)[3])(st->positionBuffer_fd + h->nL);
+  st->theta_fd = st->positionBuffer_fd + h->nL + 3 * N;
+  st->lambdaForce_d = st->forceBuffer_d;
+  st->force_d = (float(*)[3])(st->forceBuffer_d + h->nL);
+  st->thetaForce_d = st->forceBuffer_d + h->nL + 3 * N;
+  st->typeBox = false;
+  st->orthBox.x = box[0]; st->orthBox.y = box[1]; st->orthBox.z = box[2];
+  st->orthBox_f.x = (float)box[0]; st->orthBox_f.y = (float)box[1]; st->orthBox_f.z = (float)box[2];
+  {
+    double one = 1.0;
+    cudaMemcpy(st->lambda_d, &one, sizeof(double), cudaMemcpyHostToDevice);
+  }
+
+  // Potential: nonbonded tables (potential.cxx:1336-1420) and exclusions
+  pot->atomCount = N;
+  NbondPotential *nb = (NbondPotential *)malloc(sizeof(NbondPotential) * (N > 0 ? N : 1));
+  for (int i = 0; i < N; i++) {
+    nb[i].siteBlock = siteBlock[i];
+    nb[i].q = q[i];
+    nb[i].typeIdx = typeIdx[i];
+  }
+  cudaMalloc(&pot->nbonds_d, sizeof(NbondPotential) * (N > 0 ? N : 1));
+  cudaMemcpy(pot->nbonds_d, nb, sizeof(NbondPotential) * N, cudaMemcpyHostToDevice);
+  free(nb);
+  pot->vdwParameterCount = nTypes;
+  size_t vb = sizeof(VdwPotential) * nTypes * nTypes;
+  cudaMalloc(&pot->vdwParameters_d, vb);
+  cudaMemcpy(pot->vdwParameters_d, vdw, vb, cudaMemcpyHostToDevice);
+  {
+    cudaResourceDesc rd;
+    memset(&rd, 0, sizeof(rd));
+    rd.resType = cudaResourceTypeLinear;
+    rd.res.linear.devPtr = pot->vdwParameters_d;
+    rd.res.linear.desc = cudaCreateChannelDesc<float2>();
+    rd.res.linear.sizeInBytes = vb;
+    cudaTextureDesc td;
+    memset(&td, 0, sizeof(td));
+    td.readMode = cudaReadModeElementType;
+    if (cudaCreateTextureObject(&pot->vdwParameters_tex, &rd, &td, NULL) != cudaSuccess) return 2;
+  }
+  pot->exclCount = exclCount;
+  cudaMalloc(&pot->excls_d, sizeof(ExclPotential) * (exclCount > 0 ? exclCount : 1));
+  cudaMemcpy(pot->excls_d, excl, sizeof(int) * 2 * exclCount, cudaMemcpyHostToDevice);
+
+  sys->domdec = new Domdec();
+  *out = h;
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// Coordinates (host FP64, [N][3]) and lambda (host FP64 [nL]) into position_d / lambda_d.
+extern "C" int ref_set_state(ref_handle *h, const double *xyz, const double *lambda) {
+  State *st = h->st;
+  if (xyz) cudaMemcpyAsync(st->position_d, xyz, sizeof(double) * 3 * h->N, cudaMemcpyHostToDevice, h->stream);
+  if (lambda) cudaMemcpyAsync(st->lambda_d, lambda, sizeof(double) * h->nL, cudaMemcpyHostToDevice, h->stream);
+  cudaStreamSynchronize(h->stream);
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// Same from a device buffer of 3N doubles (timed trajectories).
+extern "C" int ref_set_positions_device(ref_handle *h, const double *xyz_d) {
+  cudaMemcpyAsync(h->st->position_d, xyz_d, sizeof(double) * 3 * h->N, cudaMemcpyDeviceToDevice,
+                  h->stream);
+  return 0;
+}
+
+// One step of the path: list maintenance then the force call, as the step
+// loop does it.  reset: rebuild the list (every freqDomdec steps).
+static void ref_step(ref_handle *h, int reset, int calcEnergy) {
+  System *sys = h->sys;
+  if (!h->initialized) {
+    sys->domdec->initialize(sys);  // includes the first reset_domdec
+    h->initialized = true;
+  } else {
+    sys->domdec->update_domdec(sys, reset != 0);
+  }
+  // Potential::reset_force (potential.cxx:1839-1849), nbdirect part
+  cudaMemsetAsync(sys->state->forceBuffer_d, 0, sizeof(float) * (3 * h->N + 2 * h->nL), h->stream);
+  cudaMemsetAsync(sys->domdec->localForce_d, 0, 32 * sys->domdec->maxBlocks * sizeof(float) * 3, h->stream);
+  cudaMemsetAsync(sys->state->energy_d, 0, sizeof(double) * eeend, h->stream);
+  getforce_nbdirect(sys, calcEnergy != 0);
+}
+
+extern "C" int ref_evaluate(ref_handle *h, int reset, int calcEnergy, double *grad, double *energy,
+                            double *lambdaForce) {
+  ref_step(h, reset, calcEnergy);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return 2;
+  State *st = h->st;
+  int n = 3 * h->N;
+  float *tmp = (float *)malloc(sizeof(float) * (n + h->nL));
+  cudaMemcpy(tmp, st->force_d, sizeof(float) * n, cudaMemcpyDeviceToHost);
+  for (int i = 0; i < n; i++) grad[i] = tmp[i];
+  if (lambdaForce) {
+    cudaMemcpy(tmp, st->lambdaForce_d, sizeof(float) * h->nL, cudaMemcpyDeviceToHost);
+    for (int i = 0; i < h->nL; i++) lambdaForce[i] = tmp[i];
+  }
+  free(tmp);
+  if (energy) cudaMemcpy(energy, st->energy_d + eenbdirect, sizeof(double), cudaMemcpyDeviceToHost);
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// Times `steps` steps over a device trajectory frames_d [steps][3N] (FP64),
+// rebuilding every `rebuildEvery` steps; returns the summed device time of
+// each step (events on the path's stream) in *ms.  flush_d (flushBytes) is
+// overwritten between steps, outside the timed events, to evict L2.
+extern "C" int ref_time(ref_handle *h, const double *frames_d, int steps, int rebuildEvery,
+                        int calcEnergy, void *flush_d, size_t flushBytes, double *ms) {
+  double total = 0;
+  for (int k = 0; k < steps; k++) {
+    ref_set_positions_device(h, frames_d + (size_t)k * 3 * h->N);
+    if (flush_d) cudaMemsetAsync(flush_d, k & 0xFF, flushBytes, h->stream);
+    cudaEventRecord(h->e0, h->stream);
+    ref_step(h, k % rebuildEvery == 0, calcEnergy);
+    cudaEventRecord(h->e1, h->stream);
+    cudaEventSynchronize(h->e1);
+    float t = 0;
+    cudaEventElapsedTime(&t, h->e0, h->e1);
+    total += t;
+  }
+  *ms = total;
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+extern "C" int ref_list_info(ref_handle *h, int *blocks, int *maxPartners) {
+  Domdec *d = h->sys->domdec;
+  if (blocks) *blocks = d->blockCount ? d->blockCount[1] : 0;
+  if (maxPartners) *maxPartners = d->maxPartnersPerBlock;
+  return 0;
+}

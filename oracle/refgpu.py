@@ -1,0 +1,85 @@
+"""ctypes front end of oracle/_ref/libbladeref.so: the reference's own CUDA
+direct-space path (src/nbdirect + src/domdec, unmodified) driven by
+oracle/ref/ref_harness.cu.  Comparison and golden-vector infrastructure only.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_ref", "libbladeref.so")
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(LIB_PATH)
+        p, i, f, d = C.c_void_p, C.c_int, C.c_float, C.c_double
+        L.ref_create.argtypes = [i, p, p, p, i, p, i, p, i, i, f, f, f, i, i, f, p, p]
+        L.ref_set_state.argtypes = [p, p, p]
+        L.ref_evaluate.argtypes = [p, i, i, p, p, p]
+        L.ref_time.argtypes = [p, p, i, i, i, p, C.c_size_t, p]
+        L.ref_list_info.argtypes = [p, p, p]
+        _lib = L
+    return _lib
+
+
+class RefGPU:
+    """The reference path for one synthetic System (AKMA units)."""
+
+    def __init__(self, sys):
+        self.sys = sys
+        nb = sys.nbonds
+        self.N = sys.N
+        self.nL = sys.msld.blockCount if sys.msld else 1
+        sb = np.ascontiguousarray(nb["siteBlock"], np.int32)
+        q = np.ascontiguousarray(nb["q"], np.float32)
+        t = np.ascontiguousarray(nb["typeIdx"], np.int32)
+        vdw = np.ascontiguousarray(sys.vdw, np.float32)
+        ex = np.ascontiguousarray(sys.excl, np.int32)
+        box = np.ascontiguousarray(sys.box, np.float64)
+        soft = int(bool(sys.msld and sys.msld.useSoftCore))
+        h = C.c_void_p()
+        P = lambda a: a.ctypes.data_as(C.c_void_p)
+        rc = lib().ref_create(self.N, P(sb), P(q), P(t), sys.nTypes, P(vdw), len(ex), P(ex), self.nL, soft,
+                              sys.rCut, sys.rSwitch, sys.betaEwald, sys.elecMethod, sys.vdwMethod,
+                              sys.cullPad, P(box), C.byref(h))
+        if rc != 0:
+            raise RuntimeError("reference harness: create failed")
+        self.h = h
+
+    def set_state(self, xyz=None, lam=None):
+        P = lambda a: None if a is None else np.ascontiguousarray(a, np.float64).ctypes.data_as(C.c_void_p)
+        x = None if xyz is None else np.ascontiguousarray(xyz, np.float64)
+        l = None if lam is None else np.ascontiguousarray(lam, np.float64)
+        lib().ref_set_state(self.h, P(x), P(l))
+
+    def evaluate(self, xyz=None, lam=None, reset=True, energy=True):
+        self.set_state(self.sys.xyz if xyz is None else xyz, self.sys.lambdas() if lam is None else lam)
+        g = np.zeros(3 * self.N)
+        e = np.zeros(1)
+        lf = np.zeros(self.nL)
+        rc = lib().ref_evaluate(self.h, int(reset), int(energy), g.ctypes.data_as(C.c_void_p),
+                                e.ctypes.data_as(C.c_void_p), lf.ctypes.data_as(C.c_void_p))
+        if rc != 0:
+            raise RuntimeError("reference harness: evaluate failed")
+        return {"grad": g.reshape(-1, 3), "energy": float(e[0]), "lambdaForce": lf}
+
+    def time(self, frames_d, steps, rebuild_every=10, energy=True, flush=None):
+        """Device time (ms) of `steps` steps over a torch float64 CUDA tensor [steps, 3N]."""
+        ms = C.c_double()
+        fptr = C.c_void_p(flush.data_ptr()) if flush is not None else None
+        fbytes = flush.numel() * flush.element_size() if flush is not None else 0
+        rc = lib().ref_time(self.h, C.c_void_p(frames_d.data_ptr()), int(steps), int(rebuild_every), int(energy),
+                            fptr, C.c_size_t(fbytes), C.byref(ms))
+        if rc != 0:
+            raise RuntimeError("reference harness: timing failed")
+        return ms.value
