@@ -62,7 +62,7 @@ struct Dev {
   int *atomType;           // [N]
   int *atomSiteBlock;      // [N] (site<<16)|global lambda index, 0 = environment
   float2 *ljTable;         // [nTypes*nTypes] (c12,c6)   table mode
-  float2 *ljType;          // [nTypes] (sqrt(2 eps), Rmin/2) combine mode
+  float2 *ljType;          // [nTypes] (sqrt(12 eps), Rmin/2) combine mode
   int *exclStart;          // [N+1]
   int *exclAtom;           // [E]
   // --- capacities ----------------------------------------------------------
@@ -110,6 +110,7 @@ struct PairConst {        // uniform parameters of the pair kernel
   float softR;            // soft-core radius (4 A in AKMA)
   // PME
   float mBeta2Log2e;      // -beta^2 * log2(e)
+  float pBeta;            // erfc fit parameter p times beta
   float twoBetaSqrtPi;    // 2*beta/sqrt(pi)
   // VFSWITCH
   float k6, k12, rci3, rci6, dv6, dv12;

@@ -17,6 +17,7 @@
 
 #include "bnb.h"
 #include "bnb_internal.h"
+#include "erfc_fit.h"
 #include "listbuild.h"
 #include "nbdirect.h"
 
@@ -92,6 +93,7 @@ PairConst make_const(const bnb_params &p) {
   c.beta = (float)b;
   c.softR = p.softCoreRadius;
   c.mBeta2Log2e = (float)(-b * b / std::log(2.0));
+  c.pBeta = bnb::kErfcP * (float)b;
   c.twoBetaSqrtPi = (float)(2.0 * b / std::sqrt(M_PI));
   double rc3 = rc * rc * rc, rs3 = rs * rs * rs;
   c.k6 = (float)(rc3 / (rc3 - rs3));
@@ -425,7 +427,7 @@ int bnb_set_topology(bnb_handle *h, const bnb_nbond *nbonds, const int *typeCoun
             return BNB_ERR_UNSUPPORTED;
         }
       for (int i = 0; i < t; i++)
-        ljType[typeStart[r] + i] = make_float2((float)std::sqrt(2.0 * e[i]), (float)rh[i]);
+        ljType[typeStart[r] + i] = make_float2((float)std::sqrt(12.0 * e[i]), (float)rh[i]);
       off += (size_t)t * t;
     }
   }

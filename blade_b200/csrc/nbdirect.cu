@@ -68,6 +68,20 @@ __device__ __forceinline__ bool aabb_hit(float4 imin, float4 imax, float4 jmin, 
   return acc <= c2;
 }
 
+// erfc(x) exp(x^2) as P8(t), t = 1/(1+p x): even/odd split halves the
+// dependency chain of a plain Horner evaluation.
+__device__ __forceinline__ float erfcx_poly(float t) {
+  const float t2 = t * t;
+  float pe = fmaf(kErfcC8, t2, kErfcC6);
+  pe = fmaf(pe, t2, kErfcC4);
+  pe = fmaf(pe, t2, kErfcC2);
+  pe = fmaf(pe, t2, kErfcC0);
+  float po = fmaf(kErfcC7, t2, kErfcC5);
+  po = fmaf(po, t2, kErfcC3);
+  po = fmaf(po, t2, kErfcC1);
+  return fmaf(po, t, pe);
+}
+
 __device__ __forceinline__ long long to_fix(float v) {
   return __float2ll_rn(v * kFixScaleF);
 }
@@ -86,16 +100,8 @@ __device__ __forceinline__ void pair_terms(const PairConst &pc, float r, float r
                                            float &E) {
   float fe, ee = 0.f;
   if (ELEC == 1) {  // PME real space
-    float t = rcp_approx(fmaf(kErfcP, pc.beta * r, 1.0f));
-    float p = kErfcC8;
-    p = fmaf(p, t, kErfcC7);
-    p = fmaf(p, t, kErfcC6);
-    p = fmaf(p, t, kErfcC5);
-    p = fmaf(p, t, kErfcC4);
-    p = fmaf(p, t, kErfcC3);
-    p = fmaf(p, t, kErfcC2);
-    p = fmaf(p, t, kErfcC1);
-    p = fmaf(p, t, kErfcC0);
+    float t = rcp_approx(fmaf(pc.pBeta, r, 1.0f));
+    float p = erfcx_poly(t);
     float g = ex2_approx(pc.mBeta2Log2e * r2);
     float eel = qq * (p * g) * rinv;
     fe = -fmaf(qq * pc.twoBetaSqrtPi, g, eel) * rinv;
@@ -161,16 +167,19 @@ __device__ __forceinline__ void pair_terms(const PairConst &pc, float r, float r
   E = ee + el;
 }
 
+// LJ pair coefficients.  Combination mode stores per type (sqrt(12 eps),
+// Rmin/2): e6 = 12 sqrt(eps_i eps_j), c6 = 2 eps Rmin^6 = e6 R6/6,
+// c12 = eps Rmin^12 = e6 R6^2/12 (potential.cxx:1393-1403).
 template <bool COMBINE>
 __device__ __forceinline__ void lj_params(const float2 *sLJ, int rowI, int tj, float2 ljI,
                                           float2 ljJ, float &c12, float &c6) {
   if (COMBINE) {
-    float e = ljI.x * ljJ.x;
+    float e6 = ljI.x * ljJ.x;
     float R = ljI.y + ljJ.y;
     float R2 = R * R;
     float R6 = R2 * R2 * R2;
-    c6 = e * R6;
-    c12 = 0.5f * e * R6 * R6;
+    c6 = (e6 * (1.f / 6.f)) * R6;
+    c12 = (e6 * (1.f / 12.f)) * R6 * R6;
   } else {
     float2 v = sLJ[rowI + tj];
     c12 = v.x;
@@ -182,8 +191,64 @@ struct KArgs {
   Dev d;
   PairConst pc;
   const float *lambda;     // [lamTotal] or null
-  int count;               // count in-cutoff pairs
+  int count;               // count in-cutoff pairs (energy variants only)
 };
+
+// One non-alchemical pair at r2 < rCut^2: returns (dE/dr)/r and, with
+// ENERGY, the pair energy.  PME + VFSWITCH (the production combination) is
+// written out with the switching algebra folded:
+//   VFSWITCH dE/dr * r = 6 c6 a r^-3 - 12 c12 b r^-6   (nbdirect.cu:336-346)
+// with a, b = (r^-3, r^-6) inside rSwitch and (k6 (r^-3 - rc^-3),
+// k12 (r^-6 - rc^-6)) outside; in combination mode this is
+// e6 w (a - w b) with w = Rmin^6 r^-3.  Other methods use pair_terms.
+template <int ELEC, int VDW, bool ENERGY, bool COMBINE>
+__device__ __forceinline__ float plain_pair(const PairConst &pc, float r2, float qq, const float2 *sLJ,
+                                            int rowI, int tj, float2 ljI, float2 ljJ, float &E) {
+  const float rinv = rsqrt_approx(r2);
+  const float r = r2 * rinv;
+  if (ELEC == 1 && VDW == 0) {
+    const float t = rcp_approx(fmaf(pc.pBeta, r, 1.0f));
+    const float g = ex2_approx(pc.mBeta2Log2e * r2);
+    const float pg = erfcx_poly(t) * g;
+    const float eel = qq * pg * rinv;
+    const float rinv2 = rinv * rinv;
+    const float rinv3 = rinv2 * rinv;
+    const float rinv6 = rinv3 * rinv3;
+    const bool in = r < pc.rswitch;
+    const float a = in ? rinv3 : pc.k6 * (rinv3 - pc.rci3);
+    const float b = in ? rinv6 : pc.k12 * (rinv6 - pc.rci6);
+    float flr, c12 = 0.f, c6 = 0.f;
+    if (COMBINE) {
+      const float e6 = ljI.x * ljJ.x;
+      const float R = ljI.y + ljJ.y;
+      const float R2 = R * R;
+      const float R6 = R2 * R2 * R2;
+      const float w = R6 * rinv3;
+      flr = e6 * w * fmaf(-w, b, a);
+      if (ENERGY) {
+        c6 = (e6 * (1.f / 6.f)) * R6;
+        c12 = (e6 * (1.f / 12.f)) * R6 * R6;
+      }
+    } else {
+      const float2 v = sLJ[rowI + tj];
+      c12 = v.x;
+      c6 = v.y;
+      flr = fmaf(6.f * c6 * a, rinv3, -12.f * c12 * b * rinv6);
+    }
+    if (ENERGY) {
+      const float pe = in ? fmaf(rinv6, rinv6, -pc.dv12) : b * (rinv6 - pc.rci6);
+      const float qe = in ? rinv6 - pc.dv6 : a * (rinv3 - pc.rci3);
+      E = eel + (c12 * pe - c6 * qe);
+    }
+    return (flr - fmaf(qq * pc.twoBetaSqrtPi, g, eel)) * rinv2;
+  } else {
+    float c12, c6;
+    lj_params<COMBINE>(sLJ, rowI, tj, ljI, ljJ, c12, c6);
+    float dEdr;
+    pair_terms<ELEC, VDW, ENERGY>(pc, r, r2, rinv, qq, c12, c6, dEdr, E);
+    return dEdr * rinv;
+  }
+}
 
 // j-side registers that travel with the rotation.
 template <bool COMBINE, int ALCH>
@@ -195,12 +260,12 @@ struct JRegs {
   float l;                 // lambda of b
   float fx, fy, fz, fl;
 
-  __device__ __forceinline__ void move(int src, int width) {
+  __device__ __forceinline__ void move(int src, int width, bool withMeta = true) {
     x = __shfl_sync(kFull, x, src, width);
     y = __shfl_sync(kFull, y, src, width);
     z = __shfl_sync(kFull, z, src, width);
     q = __shfl_sync(kFull, q, src, width);
-    meta = __shfl_sync(kFull, meta, src, width);
+    if (withMeta) meta = __shfl_sync(kFull, meta, src, width);
     if (COMBINE) {
       ex = __shfl_sync(kFull, ex, src, width);
       er = __shfl_sync(kFull, er, src, width);
@@ -217,6 +282,36 @@ struct JRegs {
     if (ALCH && alch) fl = __shfl_sync(kFull, fl, src, width);
   }
 };
+
+// gj rotation steps of a tile without MSLD scaling.  MASKED tiles test the
+// exclusion/diagonal row bit of the current j (its original lane travels in
+// J.meta); the others rely on far-away sentinels for empty slots.
+template <int ELEC, int VDW, bool ENERGY, bool COMBINE, bool MASKED, int ALCH>
+__device__ __forceinline__ void plain_loop(JRegs<COMBINE, ALCH> &J, const float4 &xi, uint32_t row, int gj,
+                                           int rot, const PairConst &pc, const float2 *sLJ, int rowI,
+                                           float2 ljI, float &fix, float &fiy, float &fiz, float &ei,
+                                           unsigned long long &pairs, int count) {
+#pragma unroll 4
+  for (int k = 0; k < gj; k++) {
+    const float dx = xi.x - J.x, dy = xi.y - J.y, dz = xi.z - J.z;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    bool act = r2 < pc.rc2;
+    if (MASKED) act = act && ((row >> (COMBINE ? J.meta : (J.meta >> 16))) & 1u);
+    if (act) {
+      float E = 0.f;
+      const float fs = plain_pair<ELEC, VDW, ENERGY, COMBINE>(pc, r2, xi.w * J.q, sLJ, rowI, J.meta & 0xFFFF,
+                                                              ljI, make_float2(J.ex, J.er), E);
+      fix = fmaf(fs, dx, fix); fiy = fmaf(fs, dy, fiy); fiz = fmaf(fs, dz, fiz);
+      J.fx = fmaf(-fs, dx, J.fx); J.fy = fmaf(-fs, dy, J.fy); J.fz = fmaf(-fs, dz, J.fz);
+      if (ENERGY) {
+        ei += E;
+        if (count) pairs++;
+      }
+    }
+    J.move(rot, gj, MASKED || !COMBINE);
+    J.move_forces(rot, gj, false);
+  }
+}
 
 // ---------------------------------------------------------------------------
 // The pair kernel.
@@ -268,8 +363,9 @@ __global__ void __launch_bounds__(256, 4) k_pair(KArgs A) {
     int c1 = d.candStart[iBlock + 1];
     c1 = c1 < c0 + kTilesPerWork ? c1 : c0 + kTilesPerWork;
     const int islot = 32 * iBlock + lane;
-    const float4 xi = d.xyzq[islot];
+    float4 xi = d.xyzq[islot];
     const bool iValid = d.slotAtom[islot] >= 0;
+    if (!iValid) xi.x = -1.0e18f;  // empty i slot: never within rCut of any j
     const int ti = d.slotType[islot];
     const int rowI = ti * nT;
     const float2 ljI = COMBINE ? d.ljType[ti] : make_float2(0.f, 0.f);
@@ -353,29 +449,17 @@ __global__ void __launch_bounds__(256, 4) k_pair(KArgs A) {
       if (cl >= nj) J.x = 1.0e18f;  // empty compacted slot: never within rCut
       J.fx = J.fy = J.fz = J.fl = 0.f;
       const int rot = lane + 1;
+      // Tiles without an exclusion mask and off the diagonal need no per-step
+      // mask test: empty j slots and invalid i lanes sit far outside rCut.
+      const bool masked = mIdx >= 0 || (jBlock == iBlock && code == 0);
 
       if (!alchTile) {
-#pragma unroll 4
-        for (int k = 0; k < gj; k++) {
-          const float dx = xi.x - J.x, dy = xi.y - J.y, dz = xi.z - J.z;
-          const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          const int jb = COMBINE ? J.meta : (J.meta >> 16);
-          if (((row >> jb) & 1u) && r2 < pc.rc2) {
-            float c12, c6;
-            lj_params<COMBINE>(sLJ, rowI, J.meta & 0xFFFF, ljI, make_float2(J.ex, J.er), c12, c6);
-            const float rinv = rsqrt_approx(r2);
-            const float r = r2 * rinv;
-            float dEdr, E;
-            pair_terms<ELEC, VDW, ENERGY>(pc, r, r2, rinv, xi.w * J.q, c12, c6, dEdr, E);
-            const float fs = dEdr * rinv;
-            fix = fmaf(fs, dx, fix); fiy = fmaf(fs, dy, fiy); fiz = fmaf(fs, dz, fiz);
-            J.fx = fmaf(-fs, dx, J.fx); J.fy = fmaf(-fs, dy, J.fy); J.fz = fmaf(-fs, dz, J.fz);
-            if (ENERGY) ei += E;
-            if (A.count) pairs++;
-          }
-          J.move(rot, gj);
-          J.move_forces(rot, gj, false);
-        }
+        if (masked)
+          plain_loop<ELEC, VDW, ENERGY, COMBINE, true>(J, xi, row, gj, rot, pc, sLJ, rowI, ljI, fix, fiy, fiz,
+                                                       ei, pairs, A.count);
+        else
+          plain_loop<ELEC, VDW, ENERGY, COMBINE, false>(J, xi, row, gj, rot, pc, sLJ, rowI, ljI, fix, fiy,
+                                                        fiz, ei, pairs, A.count);
       } else if (ALCH) {
         for (int k = 0; k < gj; k++) {
           const float dx = xi.x - J.x, dy = xi.y - J.y, dz = xi.z - J.z;
@@ -421,7 +505,7 @@ __global__ void __launch_bounds__(256, 4) k_pair(KArgs A) {
             fix = fmaf(fs, dx, fix); fiy = fmaf(fs, dy, fiy); fiz = fmaf(fs, dz, fiz);
             J.fx = fmaf(-fs, dx, J.fx); J.fy = fmaf(-fs, dy, J.fy); J.fz = fmaf(-fs, dz, J.fz);
             if (ENERGY) ei = fmaf(s, E, ei);
-            if (A.count) pairs++;
+            if (ENERGY && A.count) pairs++;
           }
           J.move(rot, gj);
           J.move_forces(rot, gj, true);

@@ -244,17 +244,18 @@ extern "C" int ref_evaluate(ref_handle *h, int reset, int calcEnergy, double *gr
 }
 
 // Times `steps` steps over a device trajectory frames_d [steps][3N] (FP64),
-// rebuilding every `rebuildEvery` steps; returns the summed device time of
+// rebuilding every `rebuildEvery` steps and computing the energy every
+// `energyEvery` steps (0: never); returns the summed device time of
 // each step (events on the path's stream) in *ms.  flush_d (flushBytes) is
 // overwritten between steps, outside the timed events, to evict L2.
 extern "C" int ref_time(ref_handle *h, const double *frames_d, int steps, int rebuildEvery,
-                        int calcEnergy, void *flush_d, size_t flushBytes, double *ms) {
+                        int energyEvery, void *flush_d, size_t flushBytes, double *ms) {
   double total = 0;
   for (int k = 0; k < steps; k++) {
     ref_set_positions_device(h, frames_d + (size_t)k * 3 * h->N);
     if (flush_d) cudaMemsetAsync(flush_d, k & 0xFF, flushBytes, h->stream);
     cudaEventRecord(h->e0, h->stream);
-    ref_step(h, k % rebuildEvery == 0, calcEnergy);
+    ref_step(h, k % rebuildEvery == 0, energyEvery > 0 && k % energyEvery == 0);
     cudaEventRecord(h->e1, h->stream);
     cudaEventSynchronize(h->e1);
     float t = 0;

@@ -73,12 +73,12 @@ class RefGPU:
             raise RuntimeError("reference harness: evaluate failed")
         return {"grad": g.reshape(-1, 3), "energy": float(e[0]), "lambdaForce": lf}
 
-    def time(self, frames_d, steps, rebuild_every=10, energy=True, flush=None):
+    def time(self, frames_d, steps, rebuild_every=10, energy_every=10, flush=None):
         """Device time (ms) of `steps` steps over a torch float64 CUDA tensor [steps, 3N]."""
         ms = C.c_double()
         fptr = C.c_void_p(flush.data_ptr()) if flush is not None else None
         fbytes = flush.numel() * flush.element_size() if flush is not None else 0
-        rc = lib().ref_time(self.h, C.c_void_p(frames_d.data_ptr()), int(steps), int(rebuild_every), int(energy),
+        rc = lib().ref_time(self.h, C.c_void_p(frames_d.data_ptr()), int(steps), int(rebuild_every), int(energy_every),
                             fptr, C.c_size_t(fbytes), C.byref(ms))
         if rc != 0:
             raise RuntimeError("reference harness: timing failed")
