@@ -66,6 +66,8 @@ def lib():
             "bnb_lambda_from_theta": (i, [i, p, d, p, p, p, p, p]),
             "bnb_theta_force": (i, [i, p, p, d, p, p, p, p, p, p]),
             "bnb_bias": (i, [i, p, p, i, p, p, p, p]),
+            "bnb_theta_force_f32": (i, [i, p, p, d, p, p, p, p, p, p]),
+            "bnb_bias_f32": (i, [i, p, p, i, p, p, p, p]),
             "bnb_version": (C.c_char_p, []),
         }
         for name, (res, args) in sig.items():

@@ -1,19 +1,24 @@
-// MSLD lambda maps and lambda biases (sm_100a), FP64.
+// MSLD lambda maps and lambda biases (sm_100a), computed in FP64.
 //
 // Counterparts of Msld::calc_lambda_from_theta (src/msld/msld.cu:863-921),
 // Msld::calc_thetaForce_from_lambdaForce (msld.cu:937-998) and the fixed and
 // variable lambda biases (msld.cu:1000-1153).  These are tiny per-site /
-// per-bias loops; one thread per site, block or bias term.  Energies are
-// reduced in a fixed order (warp butterfly, then one FP64 atomic per warp).
+// per-block / per-bias loops: one thread each.  Entry points come in the
+// FP64 form and, for the buffers BLaDE's State keeps in FP32 (lambda_fd,
+// theta_fd, lambdaForce_d, thetaForce_d, lambdaBias_d), an FP32-buffer form
+// that still computes in FP64.  Block-fixed flags are byte arrays, the
+// layout of the reference's bool blockFixed_d.  Energies are reduced in a
+// fixed order per warp and added with one FP64 atomic per warp.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdint.h>
 
 #include "bnb.h"
 
 namespace {
 
 __global__ void k_lambda_from_theta(int siteCount, const int *siteBound, double fnex,
-                                    const double *theta, const int *fixed, double *lambda,
+                                    const double *theta, const uint8_t *fixed, double *lambda,
                                     float *lambda_f) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= siteCount) return;
@@ -37,22 +42,23 @@ __global__ void k_lambda_from_theta(int siteCount, const int *siteBound, double 
   }
 }
 
-__global__ void k_theta_force(int blockCount, const int *lambdaSite, const int *siteBound,
-                              double fnex, const double *lambda, const double *theta,
-                              const double *lambdaForce, const int *fixed, double *thetaForce) {
+template <typename L, typename F>
+__global__ void k_theta_force(int blockCount, const int *lambdaSite, const int *siteBound, double fnex,
+                              const L *lambda, const L *theta, const F *lambdaForce, const uint8_t *fixed,
+                              F *thetaForce) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= blockCount) return;
   if (fixed && fixed[i]) return;
   int j0 = siteBound[lambdaSite[i]], j1 = siteBound[lambdaSite[i] + 1];
   double fixsum = 0, dyn = 0;
   for (int j = j0; j < j1; j++) {
-    if (fixed && fixed[j]) fixsum += lambda[j];
-    else dyn += lambda[j] * lambdaForce[j];
+    if (fixed && fixed[j]) fixsum += (double)lambda[j];
+    else dyn += (double)lambda[j] * (double)lambdaForce[j];
   }
   double fi = lambdaForce[i];
   double rfrac = 1.0 - fixsum;
   if (rfrac > 0) fi -= dyn / rfrac;
-  thetaForce[i] += fi * lambda[i] * fnex * cos(theta[i]);
+  thetaForce[i] += (F)(fi * (double)lambda[i] * fnex * cos((double)theta[i]));
 }
 
 __device__ void warp_energy(double e, double *energy) {
@@ -60,13 +66,14 @@ __device__ void warp_energy(double e, double *energy) {
   if ((threadIdx.x & 31) == 0 && e != 0.0) atomicAdd(energy, e);
 }
 
-__global__ void k_bias(int blockCount, const double *lambda, const double *fixedBias, int nVar,
-                       const bnb_varbias *vb, double *lambdaForce, double *energy) {
+template <typename L, typename F>
+__global__ void k_bias(int blockCount, const L *lambda, const L *fixedBias, int nVar,
+                       const bnb_varbias *vb, F *lambdaForce, double *energy) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   double e = 0;
   if (fixedBias && t < blockCount) {
-    atomicAdd(&lambdaForce[t], fixedBias[t]);
-    e += fixedBias[t] * lambda[t];
+    atomicAdd(&lambdaForce[t], (F)fixedBias[t]);
+    e += (double)fixedBias[t] * (double)lambda[t];
   }
   if (t < nVar) {
     bnb_varbias v = vb[t];
@@ -93,8 +100,8 @@ __global__ void k_bias(int blockCount, const double *lambda, const double *fixed
                fj = k * n * li * pow(lj, n - 1) / (li + l0); break;
       default: break;
     }
-    if (fi != 0.0) atomicAdd(&lambdaForce[v.i], fi);
-    if (fj != 0.0) atomicAdd(&lambdaForce[v.j], fj);
+    if (fi != 0.0) atomicAdd(&lambdaForce[v.i], (F)fi);
+    if (fj != 0.0) atomicAdd(&lambdaForce[v.j], (F)fj);
     e += E;
   }
   if (energy) warp_energy(e, energy);
@@ -102,10 +109,34 @@ __global__ void k_bias(int blockCount, const double *lambda, const double *fixed
 
 inline int blocks_for(int n) { return n > 0 ? (n + 255) / 256 : 1; }
 
+template <typename L, typename F>
+int theta_force(int blockCount, const int *lambdaSite, const int *siteBound, double fnex, const L *lambda,
+                const L *theta, const F *lambdaForce, const uint8_t *blockFixed, F *thetaForce, void *stream) {
+  if (blockCount < 0 || (blockCount > 0 && (!lambdaSite || !siteBound || !lambda || !theta ||
+                                            !lambdaForce || !thetaForce)))
+    return BNB_ERR_ARG;
+  if (blockCount == 0) return BNB_OK;
+  k_theta_force<L, F><<<blocks_for(blockCount), 256, 0, (cudaStream_t)stream>>>(
+      blockCount, lambdaSite, siteBound, fnex, lambda, theta, lambdaForce, blockFixed, thetaForce);
+  return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
+}
+
+template <typename L, typename F>
+int bias(int blockCount, const L *lambda, const L *fixedBias, int varCount, const bnb_varbias *varBias,
+         F *lambdaForce, double *energy, void *stream) {
+  if (blockCount < 0 || varCount < 0 || !lambda || !lambdaForce || (varCount > 0 && !varBias))
+    return BNB_ERR_ARG;
+  int n = blockCount > varCount ? blockCount : varCount;
+  if (n == 0) return BNB_OK;
+  k_bias<L, F><<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(blockCount, lambda, fixedBias, varCount,
+                                                                varBias, lambdaForce, energy);
+  return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
+}
+
 }  // namespace
 
 extern "C" int bnb_lambda_from_theta(int siteCount, const int *siteBound, double fnex,
-                                     const double *theta, const int *blockFixed, double *lambda,
+                                     const double *theta, const uint8_t *blockFixed, double *lambda,
                                      float *lambda_f, void *stream) {
   if (siteCount < 0 || (siteCount > 0 && (!siteBound || !theta || !lambda))) return BNB_ERR_ARG;
   if (siteCount == 0) return BNB_OK;
@@ -114,27 +145,27 @@ extern "C" int bnb_lambda_from_theta(int siteCount, const int *siteBound, double
   return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
 }
 
-extern "C" int bnb_theta_force(int blockCount, const int *lambdaSite, const int *siteBound,
-                               double fnex, const double *lambda, const double *theta,
-                               const double *lambdaForce, const int *blockFixed,
-                               double *thetaForce, void *stream) {
-  if (blockCount < 0 || (blockCount > 0 && (!lambdaSite || !siteBound || !lambda || !theta ||
-                                            !lambdaForce || !thetaForce)))
-    return BNB_ERR_ARG;
-  if (blockCount == 0) return BNB_OK;
-  k_theta_force<<<blocks_for(blockCount), 256, 0, (cudaStream_t)stream>>>(
-      blockCount, lambdaSite, siteBound, fnex, lambda, theta, lambdaForce, blockFixed, thetaForce);
-  return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
+extern "C" int bnb_theta_force(int blockCount, const int *lambdaSite, const int *siteBound, double fnex,
+                               const double *lambda, const double *theta, const double *lambdaForce,
+                               const uint8_t *blockFixed, double *thetaForce, void *stream) {
+  return theta_force<double, double>(blockCount, lambdaSite, siteBound, fnex, lambda, theta, lambdaForce,
+                                     blockFixed, thetaForce, stream);
 }
 
-extern "C" int bnb_bias(int blockCount, const double *lambda, const double *fixedBias,
-                        int varCount, const bnb_varbias *varBias, double *lambdaForce,
-                        double *energy, void *stream) {
-  if (blockCount < 0 || varCount < 0 || !lambda || !lambdaForce || (varCount > 0 && !varBias))
-    return BNB_ERR_ARG;
-  int n = blockCount > varCount ? blockCount : varCount;
-  if (n == 0) return BNB_OK;
-  k_bias<<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(blockCount, lambda, fixedBias, varCount,
-                                                         varBias, lambdaForce, energy);
-  return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
+extern "C" int bnb_theta_force_f32(int blockCount, const int *lambdaSite, const int *siteBound,
+                                   double fnex, const float *lambda, const float *theta,
+                                   const float *lambdaForce, const uint8_t *blockFixed, float *thetaForce,
+                                   void *stream) {
+  return theta_force<float, float>(blockCount, lambdaSite, siteBound, fnex, lambda, theta, lambdaForce,
+                                   blockFixed, thetaForce, stream);
+}
+
+extern "C" int bnb_bias(int blockCount, const double *lambda, const double *fixedBias, int varCount,
+                        const bnb_varbias *varBias, double *lambdaForce, double *energy, void *stream) {
+  return bias<double, double>(blockCount, lambda, fixedBias, varCount, varBias, lambdaForce, energy, stream);
+}
+
+extern "C" int bnb_bias_f32(int blockCount, const float *lambda, const float *fixedBias, int varCount,
+                            const bnb_varbias *varBias, float *lambdaForce, double *energy, void *stream) {
+  return bias<float, float>(blockCount, lambda, fixedBias, varCount, varBias, lambdaForce, energy, stream);
 }

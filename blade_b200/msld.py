@@ -2,7 +2,8 @@
 
 Counterparts of Msld::calc_lambda_from_theta, calc_thetaForce_from_lambdaForce
 and getforce_fixedBias/getforce_variableBias (src/msld/msld.cu:863-1153).
-Arguments are torch CUDA tensors (int32 indices, float64 values).
+Arguments are torch CUDA tensors (int32 indices, float64 values, uint8
+block-fixed flags in the layout of the reference's bool array).
 """
 from __future__ import annotations
 
@@ -33,6 +34,13 @@ def theta_force(lambda_site, site_bound, fnex, lam, theta, lambda_force, theta_f
                 stream=None):
     _lib.call("bnb_theta_force", lambda_site.numel(), _p(lambda_site), _p(site_bound), float(fnex), _p(lam),
               _p(theta), _p(lambda_force), _p(fixed), _p(theta_force_out), _s(stream))
+
+
+def theta_force_f32(lambda_site, site_bound, fnex, lam_f, theta_f, lambda_force_f, theta_force_f, fixed=None,
+                    stream=None):
+    """Same on the reference's FP32 State buffers (computed in FP64)."""
+    _lib.call("bnb_theta_force_f32", lambda_site.numel(), _p(lambda_site), _p(site_bound), float(fnex),
+              _p(lam_f), _p(theta_f), _p(lambda_force_f), _p(fixed), _p(theta_force_f), _s(stream))
 
 
 def bias(lam, fixed_bias, var_bias, lambda_force, energy=None, stream=None):

@@ -191,31 +191,43 @@ int bnb_fp32_peak(void *stream, double *flopsPerSecond);
 int bnb_domain_div(int atomCount, const float *box, int *divX, int *divY);
 
 /* ---- MSLD lambda maps and biases (stateless, device arrays) -------------- */
+/* All of them compute in FP64.  blockFixed is a byte per block (the layout
+ * of Msld::blockFixed_d, a bool array) and may be NULL. */
 /*
- * lambda_j = exp(fnex*sin(theta_j)) / sum over the site, FP64
+ * lambda_j = exp(fnex*sin(theta_j)) / sum over the site
  * (Msld::calc_lambda_from_theta, src/msld/msld.cu:863-921).  Also writes the
- * FP32 mirror lambda_f (State::lambda_fd) when non-NULL.  siteBound[sites+1],
- * blockFixed[blocks] (may be NULL): fixed blocks keep lambda = theta.
+ * FP32 mirror lambda_f (State::lambda_fd) when non-NULL.  siteBound[sites+1];
+ * fixed blocks keep lambda = theta.
  */
 int bnb_lambda_from_theta(int siteCount, const int *siteBound, double fnex,
-                          const double *theta, const int *blockFixed,
+                          const double *theta, const uint8_t *blockFixed,
                           double *lambda, float *lambda_f, void *stream);
 /*
  * dU/dtheta from dU/dlambda (Msld::calc_thetaForce_from_lambdaForce,
- * src/msld/msld.cu:937-998).  thetaForce is ADDED to.
+ * src/msld/msld.cu:937-998).  thetaForce is ADDED to.  The _f32 form takes
+ * the FP32 buffers the reference passes (lambda_fd, theta_fd, lambdaForce_d,
+ * thetaForce_d, msld.cu:987-991).
  */
 int bnb_theta_force(int blockCount, const int *lambdaSite,
                     const int *siteBound, double fnex, const double *lambda,
                     const double *theta, const double *lambdaForce,
-                    const int *blockFixed, double *thetaForce, void *stream);
+                    const uint8_t *blockFixed, double *thetaForce, void *stream);
+int bnb_theta_force_f32(int blockCount, const int *lambdaSite,
+                        const int *siteBound, double fnex, const float *lambda,
+                        const float *theta, const float *lambdaForce,
+                        const uint8_t *blockFixed, float *thetaForce, void *stream);
 /*
  * Fixed bias b_i*lambda_i and variable biases (types 1-12) on lambda
  * (Msld::getforce_fixedBias/getforce_variableBias, src/msld/msld.cu:1000-1153).
- * lambdaForce and energy (may be NULL) are ADDED to.
+ * lambdaForce and energy (may be NULL) are ADDED to.  The _f32 form takes the
+ * reference's FP32 lambda_fd / lambdaBias_d / lambdaForce_d buffers.
  */
 int bnb_bias(int blockCount, const double *lambda, const double *fixedBias,
              int varCount, const bnb_varbias *varBias, double *lambdaForce,
              double *energy, void *stream);
+int bnb_bias_f32(int blockCount, const float *lambda, const float *fixedBias,
+                 int varCount, const bnb_varbias *varBias, float *lambdaForce,
+                 double *energy, void *stream);
 
 /* Library version string. */
 const char *bnb_version(void);

@@ -120,19 +120,25 @@ def test_msld_lambda_kernels(cuda):
     rng = np.random.default_rng(2)
     th = rng.uniform(-2, 2, 11)
     th[0] = 1.0
-    fixed = np.zeros(11, np.int32)
+    fixed = np.zeros(11, np.uint8)          # bool layout of Msld::blockFixed_d
     fixed[0] = 1
     dev = lambda a: torch.from_numpy(a).cuda()
     lam = torch.zeros(11, dtype=torch.float64, device="cuda")
     lamf = torch.zeros(11, dtype=torch.float32, device="cuda")
     gmsld.lambda_from_theta(dev(bound), 5.5, dev(th), lam, lamf, dev(fixed))
-    ol = oracle.lambda_from_theta(bound, 5.5, th, fixed)
+    ol = oracle.lambda_from_theta(bound, 5.5, th, fixed.astype(np.int32))
     np.testing.assert_allclose(lam.cpu().numpy(), ol, rtol=1e-13, atol=1e-15)
     F = rng.normal(size=11)
     tf = torch.zeros(11, dtype=torch.float64, device="cuda")
     gmsld.theta_force(dev(site), dev(bound), 5.5, lam, dev(th), dev(F), tf, dev(fixed))
-    np.testing.assert_allclose(tf.cpu().numpy(), oracle.theta_force(site, bound, 5.5, ol, th, F, fixed),
+    np.testing.assert_allclose(tf.cpu().numpy(),
+                               oracle.theta_force(site, bound, 5.5, ol, th, F, fixed.astype(np.int32)),
                                rtol=1e-12, atol=1e-12)
+    # FP32-buffer form used with the reference's State buffers
+    tf32 = torch.zeros(11, dtype=torch.float32, device="cuda")
+    gmsld.theta_force_f32(dev(site), dev(bound), 5.5, lamf, lam.float().new_tensor(th.astype(np.float32)),
+                          dev(F.astype(np.float32)), tf32, dev(fixed))
+    np.testing.assert_allclose(tf32.cpu().numpy(), tf.cpu().numpy(), rtol=2e-5, atol=2e-5)
     vb = np.zeros(4, gmsld.VARBIAS_DTYPE)
     vb[0] = (1, 2, 6, 0.0, 2.0, 0)
     vb[1] = (1, 3, 8, 0.017, -1.5, 0)
