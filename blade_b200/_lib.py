@@ -68,6 +68,12 @@ def lib():
             "bnb_bias": (i, [i, p, p, i, p, p, p, p]),
             "bnb_theta_force_f32": (i, [i, p, p, d, p, p, p, p, p, p]),
             "bnb_bias_f32": (i, [i, p, p, i, p, p, p, p]),
+            "bnb_set_tuning": (i, [p, i, i]),
+            "bnb_get_tuning": (i, [p, p, p]),
+            "bnb_autotune": (i, [p, p, p, p, i, p, p]),
+            "bnb_bond_gradient": (i, [i, p, p, p, p, p, p]),
+            "bnb_langevin_vrorv": (i, [i, i, p, p, p, p, p, p, p, p, d, d, d, d, d, C.c_ulonglong, C.c_ulonglong,
+                                       p, p, p, p]),
             "bnb_version": (C.c_char_p, []),
         }
         for name, (res, args) in sig.items():

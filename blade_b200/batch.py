@@ -1,0 +1,217 @@
+"""Batched MSLD stepping: many replicas in one launch sequence under a CUDA graph.
+
+A step (the same for the batched and the one-at-a-time runs) is
+  list maintenance (rebuild every ``rebuild_every`` steps, asynchronous),
+  direct-space forces with MSLD scaling and soft core (bnb_compute),
+  harmonic bonds of the systems' covalent topology (bnb_bond_gradient),
+  dU/dlambda -> dU/dtheta (bnb_theta_force),
+  Langevin VRORV update of coordinates and theta (bnb_langevin_vrorv),
+  theta -> lambda (bnb_lambda_from_theta),
+mirroring Run::dynamics (src/run/run.cu:554-564) and State::update
+(src/update/update.cu:233-305) without PME reciprocal, angles/dihedrals and
+constraints; the bonds (TIP3P O-H and H-H included) stand in for the
+reference's bonded terms and SHAKE and keep molecules whole.  All replicas share one libbnb handle, so every kernel of a step
+covers all of them; ``capture`` records ``rebuild_every`` steps in one CUDA
+graph that is replayed.  Units are AKMA; dt is 2 fs.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from .nbdirect import NbDirect
+from . import systems
+from .systems import System
+
+KB = 0.001987191                 # kcal/mol/K (src/main/defines.h:53)
+PICOSECOND = 20.454828284385908  # AKMA time units per ps (defines.h:51)
+# Hydrogen mass repartitioning (3.024 amu per H, taken from its oxygen): the
+# step has no bonded terms or constraints, so heavier hydrogens keep the
+# coordinates' drift per list period within the pad.
+MASS_H, MASS_O, MASS_HEAVY = 3.024, 15.9994 - 2 * (3.024 - 1.008), 12.011
+THETA_MASS = 12.0                # amu A^2, the usual MSLD theta mass
+
+
+def atom_masses(s: System) -> np.ndarray:
+    """Water H/O by type index (0 = HT, 1 = OT in the generators), heavy atoms otherwise."""
+    t = s.nbonds["typeIdx"]
+    m = np.full(s.N, MASS_HEAVY)
+    m[t == 0] = MASS_H
+    m[t == 1] = MASS_O
+    return m
+
+
+def _p(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+class MsldBatch:
+    """State and step of R MSLD replicas on one GPU."""
+
+    def __init__(self, reps: list[System], dt_fs: float = 2.0, T: float = 300.0, gamma_ps: float = 1.0,
+                 seed: int = 1, rebuild_every: int = 10, energy_every: int = 10, device="cuda", tune=False):
+        import torch
+        self.torch = torch
+        self.reps = reps
+        self.dev = torch.device(device)
+        self.nb = NbDirect(reps, device=self.dev)
+        self.rebuild_every = rebuild_every
+        self.energy_every = energy_every
+        self.seed = seed
+        self.step_index = 0
+        N = self.nb.N
+        f64, f32, i32 = torch.float64, torch.float32, torch.int32
+        x = np.concatenate([s.xyz.astype(np.float64) for s in reps]).reshape(-1)
+        self.x = torch.from_numpy(x).to(self.dev)
+        self.xf = self.x.float()
+        masses = np.concatenate([atom_masses(s) for s in reps])
+        rng = np.random.default_rng(seed)
+        kT = KB * T
+        vx = rng.normal(size=(N, 3)) * np.sqrt(kT / masses)[:, None]
+        self.v = torch.from_numpy(vx.reshape(-1)).to(self.dev)
+        self.ismx = torch.from_numpy(np.repeat(1 / np.sqrt(masses), 3)).to(self.dev)
+        self.force = torch.zeros(3 * N, dtype=f64, device=self.dev)
+        bonds, prm = [], []
+        for r, s in enumerate(reps):
+            if s.bonds is not None and len(s.bonds):
+                bonds.append(s.bonds.astype(np.int64) + self.nb.starts[r])
+                prm.append(s.bond_param)
+        self.bond_start = None
+        if bonds:
+            st, pa, pr = systems.bond_csr(N, np.concatenate(bonds), np.concatenate(prm))
+            self.bond_start = torch.from_numpy(st).to(self.dev)
+            self.bond_partner = torch.from_numpy(pa).to(self.dev)
+            self.bond_param = torch.from_numpy(pr.reshape(-1)).to(self.dev)
+        # MSLD: global blocks = concatenation of each replica's blocks; block 0
+        # of every replica is its environment (site 0, lambda fixed at 1)
+        theta, bound, site, fixed = [], [0], [], []
+        site_base = 0
+        for s in reps:
+            m = s.msld
+            if m is None:
+                theta.append([0.0]); site.append([site_base]); bound.append(bound[-1] + 1)
+                fixed.append([1]); site_base += 1
+                continue
+            th = m.theta.copy()
+            th[0] = 1.0                                    # environment: fixed block, lambda = theta = 1
+            theta.append(th)
+            fx = np.zeros(m.blockCount, np.uint8)
+            fx[0] = 1
+            fixed.append(fx)
+            site.append(m.lambdaSite + site_base)
+            for k in range(1, m.siteCount + 1):
+                bound.append(bound[-1] + int(m.siteBound[k] - m.siteBound[k - 1]))
+            site_base += m.siteCount
+        self.theta = torch.from_numpy(np.concatenate(theta).astype(np.float64)).to(self.dev)
+        L = self.theta.numel()
+        assert L == self.nb.L
+        self.site_bound = torch.from_numpy(np.array(bound, np.int32)).to(self.dev)
+        self.lambda_site = torch.from_numpy(np.concatenate(site).astype(np.int32)).to(self.dev)
+        self.fixed = torch.from_numpy(np.concatenate(fixed).astype(np.uint8)).to(self.dev)
+        self.fnex = reps[0].msld.fnex if reps[0].msld else 5.5
+        ism_t = np.full(L, 1 / math.sqrt(THETA_MASS))
+        ism_t[np.concatenate(fixed).astype(bool)] = np.inf  # frozen, as fixed blocks in the reference
+        self.ismt = torch.from_numpy(ism_t).to(self.dev)
+        self.vt = torch.from_numpy(rng.normal(size=L) * math.sqrt(kT / THETA_MASS)).to(self.dev)
+        self.vt[self.fixed.bool()] = 0
+        self.lam = torch.zeros(L, dtype=f64, device=self.dev)
+        self.lamf = torch.zeros(L, dtype=f32, device=self.dev)
+        self.lforce = torch.zeros(L, dtype=f64, device=self.dev)
+        self.tforce = torch.zeros(L, dtype=f64, device=self.dev)
+        self.energy = torch.zeros(self.nb.R, dtype=f64, device=self.dev)
+        self.nan = torch.zeros(1, dtype=i32, device=self.dev)
+        self.step_counter = torch.zeros(2, dtype=torch.int64, device=self.dev)  # RNG step, blocks done
+        # integrator constants (State::alloc_leapparms2)
+        self.dt = dt_fs * 1e-3 * PICOSECOND
+        a = math.exp(-gamma_ps / PICOSECOND * self.dt)
+        self.fric = a
+        self.noise = math.sqrt((1 - a * a) * kT)
+        self._lambda_from_theta()
+        self.nb.update_domdec(self.xf, True)               # synchronous first build sizes the list
+        if tune:
+            self.tuned_ms = self.autotune()
+        self.graph = None
+
+    # -- kernels of one step ------------------------------------------------------
+    def _lambda_from_theta(self, stream=None):
+        _lib.call("bnb_lambda_from_theta", self.site_bound.numel() - 1, _p(self.site_bound), float(self.fnex),
+                  _p(self.theta), _p(self.fixed), _p(self.lam), _p(self.lamf), self._s(stream))
+
+    def _s(self, stream):
+        return C.c_void_p((stream or self.torch.cuda.current_stream()).cuda_stream)
+
+    def enqueue_step(self, k: int, stream=None):
+        s = self._s(stream)
+        nb = self.nb
+        if k % self.rebuild_every == 0:
+            nb.update_domdec(self.xf, True, asynchronous=True, stream=stream)
+        calc_e = self.energy_every > 0 and k % self.energy_every == 0
+        nb.getforce_nbdirect(self.xf, self.lamf, calc_e, force64=self.force, lambda_force64=self.lforce,
+                             energy64=self.energy if calc_e else None, stream=stream)
+        if self.bond_start is not None:
+            _lib.call("bnb_bond_gradient", self.nb.N, _p(self.bond_start), _p(self.bond_partner),
+                      _p(self.bond_param), _p(self.x), _p(self.force), s)
+        self.tforce.zero_()
+        _lib.call("bnb_theta_force", self.lambda_site.numel(), _p(self.lambda_site), _p(self.site_bound),
+                  float(self.fnex), _p(self.lam), _p(self.theta), _p(self.lforce), _p(self.fixed), _p(self.tforce), s)
+        _lib.call("bnb_langevin_vrorv", self.x.numel(), self.theta.numel(), _p(self.x), _p(self.v), _p(self.force),
+                  _p(self.ismx), _p(self.theta), _p(self.vt), _p(self.tforce), _p(self.ismt), self.dt, self.fric,
+                  self.noise, self.fric, self.noise, C.c_ulonglong(self.seed), C.c_ulonglong(0),
+                  _p(self.step_counter), _p(self.xf), _p(self.nan), s)
+        _lib.call("bnb_lambda_from_theta", self.site_bound.numel() - 1, _p(self.site_bound), float(self.fnex),
+                  _p(self.theta), _p(self.fixed), _p(self.lam), _p(self.lamf), s)
+
+    def run_eager(self, nsteps: int):
+        for k in range(nsteps):
+            self.enqueue_step(k)
+        self.step_index += nsteps
+
+    def capture(self):
+        """Record ``rebuild_every`` steps (one rebuild, one energy step) as a CUDA graph."""
+        torch = self.torch
+        side = torch.cuda.Stream(device=self.dev)
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):          # warm-up outside capture
+            for k in range(self.rebuild_every):
+                self.enqueue_step(k, stream=side)
+        torch.cuda.current_stream().wait_stream(side)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            for k in range(self.rebuild_every):
+                self.enqueue_step(k)
+        self.graph = g
+        return g
+
+    def run_graph(self, nsteps: int):
+        assert self.graph is not None and nsteps % self.rebuild_every == 0
+        for _ in range(nsteps // self.rebuild_every):
+            self.graph.replay()
+
+    def autotune(self, reps: int = 5) -> float:
+        best = C.c_float()
+        b = np.ascontiguousarray(self.nb.boxes, np.float32)
+        _lib.call("bnb_autotune", self.nb.h, _p(self.xf), _p(self.lamf), b.ctypes.data_as(C.c_void_p), reps,
+                  self._s(None), C.byref(best))
+        return best.value
+
+    def tuning(self):
+        t, c = C.c_int(), C.c_int()
+        _lib.call("bnb_get_tuning", self.nb.h, C.byref(t), C.byref(c))
+        return {"tiles_per_work": t.value, "ctas_per_sm": c.value}
+
+    def check(self):
+        st = self.nb.status()
+        nan = int(self.nan.item())
+        return st, nan
+
+    def close(self):
+        self.graph = None
+        self.nb.close()
+
+
+def ns_per_day(steps: int, seconds: float, dt_fs: float = 2.0, replicas: int = 1) -> float:
+    return replicas * steps * dt_fs * 1e-6 * 86400.0 / seconds

@@ -14,7 +14,8 @@
 namespace bnb {
 
 constexpr int kNumShifts = 14;        // own image + 13 half-shell images
-constexpr int kTilesPerWork = 8;      // candidate tiles per pair-kernel work item
+constexpr int kTilesPerWork = 8;      // default candidate tiles per pair-kernel work item
+constexpr int kMinTilesPerWork = 4;   // smallest setting (sizes the work-item capacity)
 constexpr int kMaxTableTypes = 64;    // LJ table kept in shared memory up to 64 types
 constexpr int kMaxLambdaShared = 2048;
 constexpr int kSortCap = 4096;        // column sort in shared memory up to 4096 atoms
@@ -56,6 +57,7 @@ struct Counters {
 struct Dev {
   // --- static topology (set_topology) -------------------------------------
   int N, R, nTypes, ljCombine, lamTotal;
+  int tilesPerWork;        // candidate tiles per work item (tuning knob, 4..32)
   RepInfo *rep;            // [R]
   int *atomRep;            // [N]
   float *atomQ;            // [N] charge * sqrt(kElectric)

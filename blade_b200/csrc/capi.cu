@@ -36,6 +36,7 @@ struct bnb_handle {
   size_t exclTotal = 0;
   // columns / replicas
   std::vector<RepInfo> rep;
+  std::vector<RepInfo> repDev;  // copy of what the device holds
   std::vector<int> colRep;
   int totalCols = 0;
   // capacities
@@ -44,6 +45,8 @@ struct bnb_handle {
   int lastWork = 0;
   int resTiles = 0, resMasks = 0, resWork = 0;
   bool reserveDirty = false;
+  int tilesPerWork = bnb::kTilesPerWork, ctasPerSM = 0;  // tuning (bnb_set_tuning / bnb_autotune)
+  int smCount = 0;
   bool counting = false;
   // profiling (bnb_profile)
   bool prof = false;
@@ -247,10 +250,12 @@ void estimate_capacities(bnb_handle *h, int &mb, long long &cand, long long &wor
     double perBlock = 0.75 * edge * edge * edge / (32 * invDens) + 16;
     cand += (long long)(perBlock * (n / 32 + 1)) + 14;
   }
-  work = cand / bnb::kTilesPerWork + mb + 16;
+  work = cand / bnb::kMinTilesPerWork + mb + 16;
   mask = (long long)(4 * h->exclTotal + 1024) / 32 + 64;
 }
 
+// Uploads the per-replica table only when it changed, so steady-state calls
+// issue no host-to-device copy (a requirement inside CUDA graph capture).
 int upload_rep(bnb_handle *h, cudaStream_t s) {
   for (int r = 0; r < h->R; r++) {
     h->rep[r].atomStart = h->atomStart[r];
@@ -258,7 +263,11 @@ int upload_rep(bnb_handle *h, cudaStream_t s) {
     h->rep[r].lamStart = h->lamStart.empty() ? 0 : h->lamStart[r];
     h->rep[r].lamCount = h->lamCount.empty() ? 1 : h->lamCount[r];
   }
-  return ok(cudaMemcpyAsync(h->d.rep, h->rep.data(), sizeof(RepInfo) * h->R,
+  if (h->repDev.size() == h->rep.size() &&
+      memcmp(h->repDev.data(), h->rep.data(), sizeof(RepInfo) * h->R) == 0)
+    return BNB_OK;
+  h->repDev = h->rep;
+  return ok(cudaMemcpyAsync(h->d.rep, h->repDev.data(), sizeof(RepInfo) * h->R,
                             cudaMemcpyHostToDevice, s))
              ? BNB_OK
              : BNB_ERR_CUDA;
@@ -499,6 +508,7 @@ int bnb_set_topology(bnb_handle *h, const bnb_nbond *nbonds, const int *typeCoun
   up(d.exclStart, exStart.data(), sizeof(int) * (N + 1));
   up(d.exclAtom, exAtom.data(), sizeof(int) * exAtom.size());
   if (!good) return BNB_ERR_CUDA;
+  h->repDev.clear();  // new device table: upload on the next rebuild
   h->topo = true;
   free_list(h);  // any previous list refers to the old topology
   for (auto &r : h->rep) { r.divX = -1; r.divY = -1; r.colStart = -1; }
@@ -538,6 +548,7 @@ int bnb_rebuild(bnb_handle *h, const float *position, const float *boxes, void *
   if (rc) return rc;
   const float rcull = h->p.rCut + h->p.cullPad;
   const float rcull2 = rcull * rcull;
+  h->d.tilesPerWork = h->tilesPerWork;
   for (int attempt = 0; attempt < 12; attempt++) {
     const bool rec = h->prof && h->rebN < kProfSlots;
     if (rec) cudaEventRecord(h->rebEv[2 * h->rebN], s);
@@ -554,9 +565,27 @@ int bnb_rebuild(bnb_handle *h, const float *position, const float *boxes, void *
     if (!ok(cudaStreamSynchronize(s))) return BNB_ERR_CUDA;
     int bad = c.status & bnb::kStatusListInvalid;
     if (!bad) {
-      h->listBuilt = true;
-      h->lastWork = c.workCount;
-      return BNB_OK;
+      // Keep at least 50 % headroom after a synchronous build, so that the
+      // asynchronous rebuilds that follow (graph-captured steps) absorb the
+      // drift of the coordinates without overflowing.
+      bool grow = false;
+      if (3LL * c.candCount > 2LL * h->capCand && h->capCand < kCapLimit) {
+        h->capCand = (int)std::min<long long>(2LL * c.candCount + 64, kCapLimit);
+        grow = true;
+      }
+      if (3LL * c.maskCount > 2LL * h->capMask) { h->capMask = 2 * c.maskCount + 64; grow = true; }
+      if (3LL * c.workCount > 2LL * h->capWork) { h->capWork = 2 * c.workCount + 64; grow = true; }
+      if (!grow) {
+        h->listBuilt = true;
+        h->lastWork = c.workCount;
+        return BNB_OK;
+      }
+      rc = alloc_list(h);
+      if (rc) return rc;
+      h->repDev.clear();
+      rc = upload_rep(h, s);
+      if (rc) return rc;
+      continue;
     }
     if (bad & bnb::kStatusBlockOverflow) return BNB_ERR_CAPACITY;  // cannot happen by construction
     // Grow what overflowed by 1.5x (src/domdec/cull.cu:337-375) and retry.
@@ -565,7 +594,7 @@ int bnb_rebuild(bnb_handle *h, const float *position, const float *boxes, void *
       cudaMemcpy(&needCand, h->d.cullOffset + h->maxBlocks * bnb::kNumShifts, sizeof(int),
                  cudaMemcpyDeviceToHost);
       h->capCand = (int)std::min<long long>((long long)std::max(needCand, h->capCand) * 3 / 2, kCapLimit);
-      h->capWork = std::max(h->capWork, h->capCand / bnb::kTilesPerWork + h->maxBlocks + 16);
+      h->capWork = std::max(h->capWork, h->capCand / bnb::kMinTilesPerWork + h->maxBlocks + 16);
     }
     if (bad & bnb::kStatusMaskOverflow) {
       int needMask = 0;
@@ -602,8 +631,14 @@ int bnb_compute(bnb_handle *h, const float *position, const float *lambda, const
   bnb::pack_positions(h->d, position, s);
   int alch = h->alch ? (h->p.useSoftCore ? 2 : 1) : 0;
   int work = h->lastWork > 0 ? h->lastWork : h->capWork;
-  int grid = (work + 7) / 8;
-  grid = std::max(1, std::min(grid, 148 * 8));
+  if (h->smCount == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&h->smCount, cudaDevAttrMultiProcessorCount, dev);
+  }
+  int grid = (work + 7) / 8;  // at most one work item per warp in the first round
+  const int cap = h->ctasPerSM > 0 ? h->ctasPerSM * h->smCount : 8 * h->smCount;
+  grid = std::max(1, std::min(grid, cap));
   const bool rec = h->prof && h->pairN < kProfSlots;
   if (rec) cudaEventRecord(h->pairEv[2 * h->pairN], s);
   int rc = bnb::launch_pair(h->d, h->pc, lambda, h->p.elecMethod, h->p.vdwMethod, alch,
@@ -658,6 +693,67 @@ int bnb_profile_read(bnb_handle *h, double *pairMs, int *pairLaunches, double *r
     h->launches = 0;
   }
   return BNB_OK;
+}
+
+int bnb_set_tuning(bnb_handle *h, int tilesPerWork, int ctasPerSM) {
+  if (!h || tilesPerWork < bnb::kMinTilesPerWork || tilesPerWork > 32 || ctasPerSM < 0 || ctasPerSM > 8)
+    return BNB_ERR_ARG;
+  if (tilesPerWork != h->tilesPerWork) h->listBuilt = false;  // work items must be rebuilt
+  h->tilesPerWork = tilesPerWork;
+  h->ctasPerSM = ctasPerSM;
+  return BNB_OK;
+}
+
+int bnb_get_tuning(bnb_handle *h, int *tilesPerWork, int *ctasPerSM) {
+  if (!h) return BNB_ERR_ARG;
+  if (tilesPerWork) *tilesPerWork = h->tilesPerWork;
+  if (ctasPerSM) *ctasPerSM = h->ctasPerSM;
+  return BNB_OK;
+}
+
+// Tries tiles-per-work-item x CTAs-per-SM settings on the caller's system and
+// keeps the fastest pair-kernel time (CUDA events, median of `reps`).
+int bnb_autotune(bnb_handle *h, const float *position, const float *lambda, const float *boxes,
+                 int reps, void *stream, float *bestMs) {
+  if (!h || !boxes || (h->N > 0 && !position) || reps < 1) return BNB_ERR_ARG;
+  if (!h->topo) return BNB_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  static const int kTiles[] = {4, 8, 16, 32};
+  static const int kCtas[] = {0, 2, 3};
+  bnb_outputs none;
+  memset(&none, 0, sizeof(none));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int bt = h->tilesPerWork, bc = h->ctasPerSM;
+  for (int t : kTiles) {
+    for (int c : kCtas) {
+      int rc = bnb_set_tuning(h, t, c);
+      if (!rc) rc = bnb_rebuild(h, position, boxes, stream, 0);
+      if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+      std::vector<float> ms;
+      for (int k = 0; k < reps + 2; k++) {
+        cudaEventRecord(e0, s);
+        rc = bnb_compute(h, position, lambda, boxes, 0, &none, stream);
+        cudaEventRecord(e1, s);
+        if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+        cudaEventSynchronize(e1);
+        float t_ms = 0;
+        cudaEventElapsedTime(&t_ms, e0, e1);
+        if (k >= 2) ms.push_back(t_ms);
+      }
+      std::sort(ms.begin(), ms.end());
+      float med = ms[ms.size() / 2];
+      if (med < best) { best = med; bt = t; bc = c; }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  int rc = bnb_set_tuning(h, bt, bc);
+  if (!rc) rc = bnb_rebuild(h, position, boxes, stream, 0);
+  if (bestMs) *bestMs = best;
+  return rc;
 }
 
 int bnb_reserve(bnb_handle *h, int tiles, int masks, int work) {

@@ -445,7 +445,7 @@ __global__ void k_cand_finish(Dev d) {
       int e = d.cullOffset[(b + 1) * kNumShifts];
       e = e < d.capCand ? e : d.capCand;
       s = s < d.capCand ? s : d.capCand;
-      d.workCountPerBlock[b] = (e - s + kTilesPerWork - 1) / kTilesPerWork;
+      d.workCountPerBlock[b] = (e - s + d.tilesPerWork - 1) / d.tilesPerWork;
     }
   }
   for (int b = B + t; b < d.maxBlocks; b += gridDim.x * blockDim.x) d.workCountPerBlock[b] = 0;
@@ -500,7 +500,7 @@ __global__ void k_mask_finish(Dev d) {
   if (total > d.capMask) atomicOr(&d.ctr->status, kStatusMaskOverflow);
 }
 
-// 13. Work items: (iBlock, first candidate) chunks of kTilesPerWork tiles.
+// 13. Work items: (iBlock, first candidate) chunks of d.tilesPerWork tiles.
 __global__ void k_work(Dev d) {
   const int B = d.ctr->blockCount;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -513,7 +513,7 @@ __global__ void k_work(Dev d) {
     int w0 = d.workOffset[b], nw = d.workCountPerBlock[b];
     int s = d.candStart[b];
     for (int k = 0; k < nw; k++)
-      if (w0 + k < d.capWork) d.work[w0 + k] = make_int2(b, s + k * kTilesPerWork);
+      if (w0 + k < d.capWork) d.work[w0 + k] = make_int2(b, s + k * d.tilesPerWork);
   }
 }
 

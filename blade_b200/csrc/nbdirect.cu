@@ -4,7 +4,7 @@
 // plus recull_blocks (src/domdec/recull.cu:41-122) and unpack_forces
 // (src/domdec/assign_blocks.cu:444-468), redesigned for Blackwell SIMT:
 //
-//  * Work item = one i-block x up to kTilesPerWork candidate j-tiles.  A warp
+//  * Work item = one i-block x up to tilesPerWork candidate j-tiles.  A warp
 //    recull-tests its candidates at rCut with the fresh AABBs (one lane per
 //    candidate, ballot), then walks the surviving tiles.
 //  * j-tile rotation: lane l owns i-atom l for the whole work item and holds
@@ -325,7 +325,7 @@ __device__ __forceinline__ void plain_loop(JRegs<COMBINE, ALCH> &J, const float4
 // with xor shuffles and returned to the owner lanes.
 // ---------------------------------------------------------------------------
 template <int ELEC, int VDW, int ALCH, bool ENERGY, bool COMBINE>
-__global__ void __launch_bounds__(256, 4) k_pair(KArgs A) {
+__global__ void __launch_bounds__(256, ALCH ? 3 : 4) k_pair(KArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int sIdx[8][32];
   const Dev &d = A.d;
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(256, 4) k_pair(KArgs A) {
     const int iBlock = wk.x;
     const int c0 = wk.y;
     int c1 = d.candStart[iBlock + 1];
-    c1 = c1 < c0 + kTilesPerWork ? c1 : c0 + kTilesPerWork;
+    c1 = c1 < c0 + d.tilesPerWork ? c1 : c0 + d.tilesPerWork;
     const int islot = 32 * iBlock + lane;
     float4 xi = d.xyzq[islot];
     const bool iValid = d.slotAtom[islot] >= 0;

@@ -65,6 +65,8 @@ class System:
     vdwMethod: int = 0           # VFSWITCH
     msld: Msld | None = None
     cullPad: float = 2.0
+    bonds: np.ndarray | None = None      # [B,2] int32 covalent bonds (one order), for dynamics only
+    bond_param: np.ndarray | None = None  # [B,2] float32 (kb, b0): U = kb/2 (r - b0)^2
 
     @property
     def N(self) -> int:
@@ -145,9 +147,20 @@ def chain_walk(rng, n: int, center: np.ndarray, radius: float, bond: float = 1.5
     """Self-avoiding walk of n atoms, 1.5 A bonds, confined to a sphere.
 
     Non-bonded atoms (|i-j|>2) stay >= dmin apart; ``avoid`` holds atoms the
-    walk must also keep dmin away from.  Each step proposes 24 directions at
-    once and checks them against a dense cell grid; dead ends backtrack.
+    walk must also keep dmin away from.  A walk that jams is restarted in a
+    sphere 12 % wider (up to six times).
     """
+    for _ in range(6):
+        try:
+            return _chain_walk_once(rng, n, center, radius, bond, dmin, start, avoid)
+        except RuntimeError:
+            radius *= 1.12
+    raise RuntimeError("chain_walk: could not place chain")
+
+
+def _chain_walk_once(rng, n, center, radius, bond, dmin, start, avoid) -> np.ndarray:
+    """One attempt: each step proposes 24 directions at once and checks them
+    against a dense cell grid; dead ends backtrack."""
     K, SLOTS = 24, 8
     start = np.asarray(center if start is None else start, np.float64)
     lo = np.minimum(start, center) - radius - 2 * dmin
@@ -215,6 +228,40 @@ def chain_walk(rng, n: int, center: np.ndarray, radius: float, bond: float = 1.5
             i -= 1
             remove(i, allpos[i])
     return allpos[:n].copy()
+
+
+# Bond force constants of the dynamics stand-in for bonded terms and SHAKE
+# (kb of U = kb/2 (r-b0)^2, kcal/mol/A^2): TIP3P O-H and H-H, backbone bonds.
+KB_OH, KB_HH, KB_CHAIN = 900.0, 200.0, 600.0
+
+
+def chain_bonds(first: int, n: int) -> np.ndarray:
+    a = first + np.arange(n - 1)
+    return np.stack([a, a + 1], 1).astype(np.int32)
+
+
+def water_bonds(first: int, nwat: int) -> tuple[np.ndarray, np.ndarray]:
+    """O-H1, O-H2, H1-H2 of each water and their force constants."""
+    o = first + 3 * np.arange(nwat)
+    b = np.concatenate([np.stack([o, o + 1], 1), np.stack([o, o + 2], 1), np.stack([o + 1, o + 2], 1)])
+    kb = np.repeat([KB_OH, KB_OH, KB_HH], nwat)
+    return b.astype(np.int32), kb
+
+
+def with_bond_lengths(xyz: np.ndarray, bonds: np.ndarray, kb: np.ndarray) -> np.ndarray:
+    """(kb, b0) per bond with b0 the bond's length in ``xyz``."""
+    b0 = np.linalg.norm(xyz[bonds[:, 0]].astype(np.float64) - xyz[bonds[:, 1]], axis=1)
+    return np.stack([kb, b0], 1).astype(np.float32)
+
+
+def bond_csr(N: int, bonds: np.ndarray, param: np.ndarray):
+    """Per-atom bond lists (both ends of every bond), stable in bond order."""
+    b = np.concatenate([bonds, bonds[:, ::-1]]).astype(np.int64)
+    prm = np.concatenate([param, param]).astype(np.float32)
+    order = np.argsort(b[:, 0], kind="stable")
+    start = np.zeros(N + 1, np.int64)
+    np.add.at(start, b[:, 0] + 1, 1)
+    return np.cumsum(start).astype(np.int32), b[order, 1].astype(np.int32), np.ascontiguousarray(prm[order])
 
 
 def chain_excl(first: int, n: int) -> np.ndarray:
@@ -302,16 +349,48 @@ def chain_in_water(seed: int = 2, box: float = 62.23, n_chain: int = 2489, n_wat
                   rCut, rSwitch, beta)
 
 
-def _add_sites(rng, sys_xyz_parts, anchors: np.ndarray, subs_per_site, box: float):
-    """Grow substituents at each anchor; returns atoms, per-atom (site, block), exclusions."""
+def _nearby(points: np.ndarray | None, center: np.ndarray, cut: float, box: float) -> np.ndarray | None:
+    """Minimum images of ``points`` within ``cut`` of ``center``."""
+    if points is None or len(points) == 0:
+        return None
+    d = points - center
+    d -= box * np.round(d / box)
+    keep = (d * d).sum(1) < cut * cut
+    return center + d[keep] if keep.any() else None
+
+
+def _add_sites(rng, fixed_atoms, anchors: np.ndarray, subs_per_site, box: float, dmin: float = 2.2,
+               avoid_sites: bool = True, outward: np.ndarray | None = None):
+    """Grow substituents at each anchor; returns atoms, per-atom (site, block), exclusions.
+
+    Substituents of one site overlap each other (they are alternatives and
+    mutually excluded); they keep ``dmin`` from ``fixed_atoms`` (the solute)
+    and, with ``avoid_sites``, from the substituents of the other sites, with
+    which they interact.  ``outward`` (unit vectors, one per site) moves the
+    walks' sphere 4 A off the anchor, away from the solute.
+    """
     atoms, site_block, bonds_excl, site_members = [], [], [], []
     block = 1
     offset = 0
+    other = np.zeros((0, 3))
     for s, (anc, nsub) in enumerate(zip(anchors, subs_per_site), start=1):
         members = []
+        site_atoms = []
+        # with an outward direction, the walks' sphere sits beside the anchor
+        out = None if outward is None else outward[s - 1]
+        center = anc if out is None else anc + 4.0 * out
+        near = [_nearby(fixed_atoms, center, 16.0, box)] + ([_nearby(other, center, 16.0, box)] if avoid_sites else [])
+        near = [a for a in near if a is not None]
+        avoid = np.concatenate(near) if near else None
         for _ in range(nsub):
             n = int(rng.integers(8, 16))
-            walk = chain_walk(rng, n, anc, 6.0, start=anc + rng.normal(0, 0.3, 3))
+            start = anc + rng.normal(0, 0.3, 3) if out is None else anc + 2.0 * out + rng.normal(0, 0.3, 3)
+            for t in range(200):                       # a start point clear of the avoided atoms
+                if avoid is None or ((avoid - start) ** 2).sum(1).min() >= dmin * dmin:
+                    break
+                start = center + rng.normal(0, 0.6 + 0.02 * t, 3)
+            walk = chain_walk(rng, n, center, 6.0, start=start, avoid=avoid)
+            site_atoms.append(walk)
             idx = offset + np.arange(n)
             atoms.append(walk)
             site_block += [(s, block)] * n
@@ -320,6 +399,7 @@ def _add_sites(rng, sys_xyz_parts, anchors: np.ndarray, subs_per_site, box: floa
             offset += n
             block += 1
         site_members.append(members)
+        other = np.concatenate([other] + site_atoms)
     mut = []
     for members in site_members:
         for a in range(len(members)):
@@ -362,7 +442,8 @@ def msld_water(seed: int = 3, sites: int = 3, subs: int = 4, clear: float = 2.2)
         dd = np.sqrt((d ** 2).sum(-1)) + 1e9 * np.eye(sites)
         if dd.min() >= 9.0:
             break
-    subs_xyz, sb, sub_excl, nblock = _add_sites(rng, None, anchors, [subs] * sites, float(base.box[0]))
+    subs_xyz, sb, sub_excl, nblock = _add_sites(rng, None, anchors, [subs] * sites, float(base.box[0]),
+                                                avoid_sites=False)
     from scipy.spatial import cKDTree
     tree = cKDTree(np.mod(subs_xyz, base.box[0]), boxsize=float(base.box[0]))
     d, _ = tree.query(np.mod(base.xyz.astype(np.float64), base.box[0]), k=1)
@@ -402,9 +483,15 @@ def msld_chain(seed: int, n_atoms: int, n_sites: int, subs_per_site, rCut=12.0, 
     center = np.full(3, box / 2)
     radius = (3 * n_chain / (4 * math.pi * 0.06)) ** (1 / 3)
     chain = chain_walk(rng, n_chain, center, radius)
-    anchors_idx = rng.choice(np.arange(5, n_chain - 5), n_sites, replace=False)
-    anchors = chain[anchors_idx] + rng.normal(0, 1.0, (n_sites, 3))
-    subs_xyz, sb, sub_excl, nblock = _add_sites(rng, None, anchors, subs_per_site, box)
+    # sites on surface atoms of the chain globule, grown outward into the water
+    rad = np.linalg.norm(chain - chain.mean(0), axis=1)
+    surface = np.arange(5, n_chain - 5)
+    surface = surface[rad[surface] >= np.quantile(rad[surface], 0.8)]
+    anchors_idx = rng.choice(surface, n_sites, replace=False)
+    anchors = chain[anchors_idx]
+    outward = anchors - chain.mean(0)
+    outward /= np.linalg.norm(outward, axis=1, keepdims=True)
+    subs_xyz, sb, sub_excl, nblock = _add_sites(rng, chain, anchors, subs_per_site, box, outward=outward)
     solute = np.concatenate([chain, subs_xyz])
     ns = len(subs_xyz)
     n_wat = max(0, (n_atoms - len(solute)) // 3)
@@ -428,8 +515,13 @@ def msld_chain(seed: int, n_atoms: int, n_sites: int, subs_per_site, rCut=12.0, 
     nbd["typeIdx"][ns + n_chain:] = np.tile(np.int32([1, 0, 0]), n_wat)
     excl = np.concatenate([sub_excl, chain_excl(ns, n_chain), water_excl(ns + n_chain, n_wat)])
     msld = _msld_layout(rng, list(subs_per_site))
+    sizes = np.bincount(sbs[:, 1])[1:]
+    firsts = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+    wb, wkb = water_bonds(ns + n_chain, n_wat)
+    bonds = np.concatenate([chain_bonds(f, n) for f, n in zip(firsts, sizes)] + [chain_bonds(ns, n_chain), wb])
+    kb = np.concatenate([np.full(len(bonds) - len(wb), KB_CHAIN), wkb])
     return System(f"msld_chain_{N}", xyz, np.float32([box] * 3), nbd, vdw_table(eps, rh), excl,
-                  rCut, rSwitch, beta, msld=msld)
+                  rCut, rSwitch, beta, msld=msld, bonds=bonds, bond_param=with_bond_lengths(xyz, bonds, kb))
 
 
 def batch_replicas(n_rep: int = 64, seed: int = 4, n_min: int = 3000, n_max: int = 30000):

@@ -229,6 +229,54 @@ int bnb_bias_f32(int blockCount, const float *lambda, const float *fixedBias,
                  int varCount, const bnb_varbias *varBias, float *lambdaForce,
                  double *energy, void *stream);
 
+/* ---- batched stepping: tuning and integrator ----------------------------- */
+/*
+ * Tuning knobs of the pair kernel: candidate tiles per work item (4..32) and
+ * CTAs per SM of the persistent grid (0 = as many as fit).  A changed tile
+ * count takes effect at the next bnb_rebuild.  No reference counterpart.
+ */
+int bnb_set_tuning(bnb_handle *h, int tilesPerWork, int ctasPerSM);
+int bnb_get_tuning(bnb_handle *h, int *tilesPerWork, int *ctasPerSM);
+/*
+ * Autotuner: times every (tiles per work item in {4,8,16,32}) x (CTAs per SM
+ * in {auto,2,3}) setting on the caller's coordinates (median of `reps`
+ * evaluations, CUDA events), keeps the fastest and rebuilds the list with it.
+ * Synchronises.  bestMs: the kept setting's pair-evaluation time.
+ */
+int bnb_autotune(bnb_handle *h, const float *position, const float *lambda,
+                 const float *boxes, int reps, void *stream, float *bestMs);
+/*
+ * Harmonic bond gradient, U = sum_bonds kb/2 (r - b0)^2, the bond form of
+ * the reference's bonded kernel (src/bonded/bonded.cu:83-112, without its
+ * soft-bond branch): adds dU/dx to grad (FP64, [3n]).  Bonds are given per
+ * atom as a CSR: for atom a, entries start[a]..start[a+1]-1 of partner and
+ * kbB0 (float pairs kb, b0), every bond listed from both ends.  Bonded atoms
+ * must be stored as one periodic image (no minimum image is taken).  The
+ * batched MSLD step uses it in place of the reference's bonded terms and
+ * constraints, which are not part of the direct-space path.
+ */
+int bnb_bond_gradient(int n, const int *start, const int *partner, const float *kbB0, const double *x,
+                      double *grad, void *stream);
+/*
+ * Langevin VRORV step of nx coordinates and nt theta values (FP64 state),
+ * the scheme of State::update (src/update/update.cu:233-305):
+ *   v -= dt ism^2 dU/dx;  x += dt/2 v;  v = a v + b ism xi;  x += dt/2 v
+ * with (a, b) = (friction, noise) = (exp(-gamma dt), sqrt((1-a^2) kT))
+ * separately for coordinates and theta (State::alloc_leapparms2), ism =
+ * 1/sqrt(mass) (non-finite: frozen).  xi are counter-based Gaussian numbers
+ * from (seed, step + *stepCounter, index); stepCounter (device, 2 x u64, may
+ * be NULL) is advanced by one per call, so a CUDA graph replaying the call
+ * draws new numbers each time.  x_f (may be NULL) receives the FP32 mirror of
+ * x (State::set_fd); nanFlag (may be NULL) is raised on a non-finite velocity.
+ */
+int bnb_langevin_vrorv(int nx, int nt, double *x, double *v, const double *fx,
+                       const double *ismx, double *theta, double *vtheta,
+                       const double *ftheta, const double *ismtheta, double dt,
+                       double frictionX, double noiseX, double frictionTheta,
+                       double noiseTheta, unsigned long long seed,
+                       unsigned long long step, unsigned long long *stepCounter,
+                       float *x_f, int *nanFlag, void *stream);
+
 /* Library version string. */
 const char *bnb_version(void);
 
