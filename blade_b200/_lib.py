@@ -16,7 +16,7 @@ BNB_OK, BNB_ERR_ARG, BNB_ERR_CUDA, BNB_ERR_CAPACITY, BNB_ERR_UNSUPPORTED, BNB_ER
 BNB_ASYNC = 1
 STATUS_BLOCK_OVERFLOW, STATUS_TILE_OVERFLOW, STATUS_MASK_OVERFLOW, STATUS_WORK_OVERFLOW, STATUS_NONFINITE = 1, 2, 4, 8, 16
 _ERRORS = {1: "bad argument", 2: "CUDA error", 3: "list capacity exceeded", 4: "unsupported",
-           5: "call order", 6: "device status"}
+           5: "call order", 6: "device status", 7: "size above the fixed limit"}
 
 
 class BnbError(RuntimeError):
@@ -71,6 +71,7 @@ def lib():
             "bnb_set_tuning": (i, [p, i, i]),
             "bnb_get_tuning": (i, [p, p, p]),
             "bnb_autotune": (i, [p, p, p, p, i, p, p]),
+            "bnb_nbdirect_noalloc": (i, [p, i, p, p, p, i, p, p, p, i, p, p]),
             "bnb_bond_gradient": (i, [i, p, p, p, p, p, p]),
             "bnb_langevin_vrorv": (i, [i, i, p, p, p, p, p, p, p, p, d, d, d, d, d, C.c_ulonglong, C.c_ulonglong,
                                        p, p, p, p]),

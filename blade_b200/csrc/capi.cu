@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -849,3 +850,88 @@ int bnb_pair_count(bnb_handle *h, void *stream, unsigned long long *pairs) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// bnb_nbdirect_noalloc: the all-pairs variant of the pair kernel for one small
+// system, for callers that may not allocate device memory at all -- not even
+// once, to create a handle.  Examples: an engine that has handed all of the
+// device's memory to its own pool before it loads this library, or a caller
+// that steps while other streams run and cannot accept the device-wide
+// synchronisation that cudaMalloc and cudaFree may bring.  The kernel's only
+// scratch, its fixed-point accumulators, is the fixed array below; every
+// other buffer is the caller's.
+// ---------------------------------------------------------------------------
+namespace {
+// [3 * BNB_NOALLOC_MAX_ATOMS] dU/dx component planes, then the energy (and
+// padding): about 98 KB, held by every device that loads this library until
+// the process exits.
+constexpr int kNoallocScratch = 3 * BNB_NOALLOC_MAX_ATOMS + 32;
+constexpr int kNoallocDevices = 64;
+long long *g_noallocPtr[kNoallocDevices];  // device address of the array, per device
+std::mutex g_noallocLock;
+}  // namespace
+
+static __device__ __align__(256) long long g_noallocScratch[kNoallocScratch];
+
+namespace {
+// Set-up, once per device, with that device current.  In host code the name
+// g_noallocScratch is only a host-side stand-in for the device array, never
+// an address a kernel may use; the device address comes from
+// cudaGetSymbolAddress and is cached per device.
+int noalloc_scratch(long long **out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return BNB_ERR_CUDA;
+  if (dev < 0 || dev >= kNoallocDevices) return BNB_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_noallocLock);
+  if (!g_noallocPtr[dev]) {
+    long long *p = nullptr;
+    if (cudaGetSymbolAddress((void **)&p, g_noallocScratch) != cudaSuccess || !p) return BNB_ERR_CUDA;
+    g_noallocPtr[dev] = p;
+  }
+  *out = g_noallocPtr[dev];
+  return BNB_OK;
+}
+}  // namespace
+
+extern "C" int bnb_nbdirect_noalloc(const bnb_params *p, int atomCount, const float *position,
+                                    const float *box, const bnb_nbond *nbonds, int typeCount,
+                                    const bnb_vdw *vdw, const int *exclStart, const int *exclAtom,
+                                    int calcEnergy, const bnb_outputs *out, void *stream) {
+  if (!p || !box || !out || atomCount < 0 || typeCount < 0) return BNB_ERR_ARG;
+  if (atomCount > BNB_NOALLOC_MAX_ATOMS) return BNB_ERR_TOO_LARGE;
+  if (atomCount > 0 && (!position || !nbonds || !vdw || typeCount < 1 || !exclStart || !exclAtom))
+    return BNB_ERR_ARG;
+  if (p->elecMethod < 0 || p->elecMethod > 2 || p->vdwMethod < 0 || p->vdwMethod > 2) return BNB_ERR_ARG;
+  if (!(p->rCut > 0) || !(p->rSwitch > 0) || p->rSwitch > p->rCut) return BNB_ERR_ARG;
+  for (int k = 0; k < 3; k++)  // minimum image: one image of each pair inside the cutoff
+    if (!(box[k] > 0) || 2.0f * p->rCut > box[k]) return BNB_ERR_ARG;
+  long long *scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  // The array keeps whatever the last call left; clear the part this call
+  // accumulates into (three planes of atomCount entries and the energy).
+  for (int k = 0; k < 3; k++)
+    if (atomCount > 0 &&
+        cudaMemsetAsync(scratch + (size_t)k * BNB_NOALLOC_MAX_ATOMS, 0, sizeof(long long) * atomCount, s) !=
+            cudaSuccess)
+      return BNB_ERR_CUDA;
+  if (cudaMemsetAsync(scratch + 3 * BNB_NOALLOC_MAX_ATOMS, 0, sizeof(long long), s) != cudaSuccess)
+    return BNB_ERR_CUDA;
+  bnb::AllPairsArgs a{};
+  a.pc = make_const(*p);
+  a.N = atomCount;
+  a.nTypes = typeCount;
+  a.stride = BNB_NOALLOC_MAX_ATOMS;
+  a.sqrtK = std::sqrt(p->kElectric);
+  a.box = make_float3(box[0], box[1], box[2]);
+  a.boxInv = make_float3(1.0f / box[0], 1.0f / box[1], 1.0f / box[2]);
+  a.x = position;
+  a.nb = nbonds;
+  a.vdw = vdw;
+  a.exclStart = exclStart;
+  a.exclAtom = exclAtom;
+  a.accF = scratch;
+  a.accE = scratch + 3 * BNB_NOALLOC_MAX_ATOMS;
+  return bnb::launch_allpairs(a, *out, p->elecMethod, p->vdwMethod, calcEnergy != 0, s);
+}

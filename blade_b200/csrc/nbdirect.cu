@@ -637,6 +637,136 @@ void launch_ev(const KArgs &a, int alch, bool energy, bool combine, int grid, si
 #undef BNB_L
 }
 
+// ---------------------------------------------------------------------------
+// All-pairs variant for one small periodic system (bnb_nbdirect_noalloc): no
+// block list; every 32x32 tile of atom blocks (J >= I) is visited by one warp
+// with minimum-image distances.  Lane l keeps atom 32I+l; the j data and the
+// j-force accumulators rotate one lane per step, so after 32 steps every lane
+// holds its own j atom again and adds its total once.  The pair physics is
+// pair_terms (the general path of the list kernel), with table LJ
+// coefficients read from global memory.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool excluded_sorted(const int *ex, int lo, int hi, int j) {
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    const int v = ex[mid];
+    if (v == j) return true;
+    if (v < j) lo = mid + 1;
+    else hi = mid;
+  }
+  return false;
+}
+
+template <int ELEC, int VDW, bool ENERGY>
+__global__ void __launch_bounds__(128) k_allpairs(AllPairsArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int I = blockIdx.y;
+  const int J = blockIdx.x * 4 + (threadIdx.x >> 5);
+  const int nb = (a.N + 31) >> 5;
+  if (J < I || J >= nb) return;  // uniform per warp
+  const PairConst &pc = a.pc;
+  const int i = 32 * I + lane;
+  const bool iv = i < a.N;
+  float xi = 0.f, yi = 0.f, zi = 0.f, qi = 0.f;
+  int ti = 0, e0 = 0, e1 = 0;
+  if (iv) {
+    xi = a.x[3 * i]; yi = a.x[3 * i + 1]; zi = a.x[3 * i + 2];
+    const bnb_nbond n = a.nb[i];
+    qi = n.q * a.sqrtK;
+    ti = n.typeIdx;
+    e0 = a.exclStart[i];
+    e1 = a.exclStart[i + 1];
+  }
+  const int j0 = 32 * J + lane;
+  float xj = 0.f, yj = 0.f, zj = 0.f, qj = 0.f;
+  int tj = 0;
+  if (j0 < a.N) {
+    xj = a.x[3 * j0]; yj = a.x[3 * j0 + 1]; zj = a.x[3 * j0 + 2];
+    const bnb_nbond n = a.nb[j0];
+    qj = n.q * a.sqrtK;
+    tj = n.typeIdx;
+  }
+  float fix = 0.f, fiy = 0.f, fiz = 0.f, fjx = 0.f, fjy = 0.f, fjz = 0.f, e = 0.f;
+  const int src = (lane + 1) & 31;
+  for (int k = 0; k < 32; ++k) {
+    const int jl = (lane + k) & 31;
+    const int j = 32 * J + jl;
+    if (iv && j < a.N && (J != I || jl > lane)) {
+      float dx = xi - xj, dy = yi - yj, dz = zi - zj;
+      dx -= a.box.x * rintf(dx * a.boxInv.x);
+      dy -= a.box.y * rintf(dy * a.boxInv.y);
+      dz -= a.box.z * rintf(dz * a.boxInv.z);
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      if (r2 < pc.rc2 && !excluded_sorted(a.exclAtom, e0, e1, j)) {
+        const float rinv = rsqrt_approx(r2);
+        const float r = r2 * rinv;
+        const bnb_vdw v = a.vdw[ti * a.nTypes + tj];
+        float dEdr = 0.f, E = 0.f;
+        pair_terms<ELEC, VDW, ENERGY>(pc, r, r2, rinv, qi * qj, v.c12, v.c6, dEdr, E);
+        const float sc = dEdr * rinv;
+        fix = fmaf(sc, dx, fix); fiy = fmaf(sc, dy, fiy); fiz = fmaf(sc, dz, fiz);
+        fjx = fmaf(-sc, dx, fjx); fjy = fmaf(-sc, dy, fjy); fjz = fmaf(-sc, dz, fjz);
+        if (ENERGY) e += E;
+      }
+    }
+    xj = __shfl_sync(0xFFFFFFFFu, xj, src);
+    yj = __shfl_sync(0xFFFFFFFFu, yj, src);
+    zj = __shfl_sync(0xFFFFFFFFu, zj, src);
+    qj = __shfl_sync(0xFFFFFFFFu, qj, src);
+    tj = __shfl_sync(0xFFFFFFFFu, tj, src);
+    fjx = __shfl_sync(0xFFFFFFFFu, fjx, src);
+    fjy = __shfl_sync(0xFFFFFFFFu, fjy, src);
+    fjz = __shfl_sync(0xFFFFFFFFu, fjz, src);
+  }
+  const int S = a.stride;
+  if (iv) {
+    red_add(&a.accF[i], to_fix(fix));
+    red_add(&a.accF[S + i], to_fix(fiy));
+    red_add(&a.accF[2 * S + i], to_fix(fiz));
+  }
+  if (j0 < a.N) {
+    red_add(&a.accF[j0], to_fix(fjx));
+    red_add(&a.accF[S + j0], to_fix(fjy));
+    red_add(&a.accF[2 * S + j0], to_fix(fjz));
+  }
+  if (ENERGY) {
+    long long ef = to_fix(e);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ef += __shfl_xor_sync(0xFFFFFFFFu, ef, o);
+    if (lane == 0 && ef != 0) red_add(a.accE, ef);
+  }
+}
+
+// Converts the all-pairs accumulators to the outputs (bnb_compute's output
+// semantics) and writes every entry it read back to zero.
+__global__ void k_allpairs_finalize(AllPairsArgs a, bnb_outputs o) {
+  const double inv = 1.0 / kFixScale;
+  const int S = a.stride;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < a.N; t += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const long long v = a.accF[k * S + t];
+      a.accF[k * S + t] = 0;
+      const double f = (double)v * inv;
+      if (o.force64) o.force64[3 * t + k] = f;
+      if (o.force && v) o.force[3 * t + k] += (float)f;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const long long v = *a.accE;
+    *a.accE = 0;
+    const double en = (double)v * inv;
+    if (o.energy64) *o.energy64 = en;
+    if (o.energy) *o.energy += en;
+  }
+}
+
+template <int ELEC, int VDW>
+void launch_allpairs_ev(const AllPairsArgs &a, bool energy, dim3 grid, cudaStream_t s) {
+  if (energy) k_allpairs<ELEC, VDW, true><<<grid, 128, 0, s>>>(a);
+  else k_allpairs<ELEC, VDW, false><<<grid, 128, 0, s>>>(a);
+}
+
 }  // namespace
 
 int launch_pair(const Dev &d, const PairConst &pc, const float *lambda, int elec, int vdw,
@@ -667,6 +797,27 @@ void launch_finalize(const Dev &d, const bnb_outputs &o, cudaStream_t s) {
   if (grid > 148 * 8) grid = 148 * 8;
   if (grid < 1) grid = 1;
   k_finalize<<<grid, 256, 0, s>>>(d, o);
+}
+
+int launch_allpairs(const AllPairsArgs &a, const bnb_outputs &o, int elec, int vdw, bool energy,
+                    cudaStream_t s) {
+  const int nb = (a.N + 31) / 32;
+  const dim3 grid((nb + 3) / 4, nb);
+  if (nb > 0) switch (elec * 3 + vdw) {
+    case 0: launch_allpairs_ev<0, 0>(a, energy, grid, s); break;
+    case 1: launch_allpairs_ev<0, 1>(a, energy, grid, s); break;
+    case 2: launch_allpairs_ev<0, 2>(a, energy, grid, s); break;
+    case 3: launch_allpairs_ev<1, 0>(a, energy, grid, s); break;
+    case 4: launch_allpairs_ev<1, 1>(a, energy, grid, s); break;
+    case 5: launch_allpairs_ev<1, 2>(a, energy, grid, s); break;
+    case 6: launch_allpairs_ev<2, 0>(a, energy, grid, s); break;
+    case 7: launch_allpairs_ev<2, 1>(a, energy, grid, s); break;
+    case 8: launch_allpairs_ev<2, 2>(a, energy, grid, s); break;
+    default: return BNB_ERR_ARG;
+  }
+  if (cudaGetLastError() != cudaSuccess) return BNB_ERR_CUDA;
+  k_allpairs_finalize<<<a.N > 0 ? (a.N + 255) / 256 : 1, 256, 0, s>>>(a, o);
+  return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
 }
 
 }  // namespace bnb

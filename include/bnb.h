@@ -30,6 +30,7 @@ extern "C" {
 #define BNB_ERR_UNSUPPORTED 4  /* feature outside this build (see message)   */
 #define BNB_ERR_STATE 5        /* call order (e.g. compute before rebuild)   */
 #define BNB_ERR_DEVICE 6       /* device status word reports a failure       */
+#define BNB_ERR_TOO_LARGE 7    /* size above a fixed limit of this build     */
 
 /* ---- device status bits (bnb_status) ------------------------------------ */
 #define BNB_STATUS_BLOCK_OVERFLOW 1
@@ -135,6 +136,56 @@ typedef struct {
 int bnb_compute(bnb_handle *h, const float *position, const float *lambda,
                 const float *boxes, int calcEnergy, const bnb_outputs *out,
                 void *stream);
+
+/*
+ * All-pairs direct space of ONE small periodic system, allocating nothing.
+ * No counterpart in the reference, whose direct space always runs on the
+ * Domdec block list (getforce_nbdirect, src/nbdirect/nbdirect.cu:574).
+ *
+ * For callers that may not allocate device memory at all -- not even once,
+ * to create a handle -- such as an engine that has given the device's whole
+ * memory to its own pool, or one that steps while other streams run and
+ * cannot accept the device-wide synchronisation that cudaMalloc/cudaFree may
+ * bring.  No handle: every input and output is the caller's, and the only
+ * scratch (the fixed-point force and energy accumulators) is a fixed array
+ * of about 98 KB inside this library, which every device that loads the
+ * library holds until the process exits.
+ *
+ * Physics: bnb_compute's for atoms outside any MSLD site (siteBlock is not
+ * read: every pair is scaled by 1), exclusions skipped, pairs with
+ * r^2 < rCut^2 under the minimum image.  The block list is replaced by
+ * every pair of atoms, so the cost grows as atomCount^2.
+ *   p        host: methods, rCut, rSwitch, betaEwald, kElectric (cullPad and
+ *            the soft-core fields are not used)
+ *   position device float [3*atomCount]; box host float [3] orthorhombic
+ *            edges, each at least 2*rCut (else BNB_ERR_ARG)
+ *   nbonds   device [atomCount], typeIdx in [0, typeCount);
+ *   vdw      device [typeCount*typeCount] table
+ *   exclStart device int [atomCount+1], exclAtom device int: the excluded
+ *            partners of atom a are exclAtom[exclStart[a]..exclStart[a+1]-1],
+ *            sorted ascending, every pair listed from both ends
+ *   out      as bnb_compute (force, energy ADDED; force64, energy64
+ *            OVERWRITTEN; the energy arrays have one entry; the lambda
+ *            outputs are not written)
+ *
+ * Limit: atomCount <= BNB_NOALLOC_MAX_ATOMS; a larger system returns
+ * BNB_ERR_TOO_LARGE and launches nothing (use a handle for it).
+ * Set-up: the first call on each device looks up the device address of the
+ * scratch array with that device current (cudaGetSymbolAddress; this may
+ * also load the library's device code on that device); make that first call
+ * before any stream capture begins.  Later calls on the device reuse it.
+ * Scratch state: the array keeps what the last call left in it; each call
+ * first clears, on its stream, the entries it accumulates into.
+ * Concurrency: all calls on one device share the one array.  Calls that may
+ * overlap on the GPU (different streams without an ordering event, several
+ * host threads) race on it and give wrong results; order them on one stream
+ * or with events.
+ */
+#define BNB_NOALLOC_MAX_ATOMS 4096
+int bnb_nbdirect_noalloc(const bnb_params *p, int atomCount, const float *position,
+                         const float *box, const bnb_nbond *nbonds, int typeCount,
+                         const bnb_vdw *vdw, const int *exclStart, const int *exclAtom,
+                         int calcEnergy, const bnb_outputs *out, void *stream);
 
 /*
  * Sets list capacities (candidate tiles, 32-row exclusion masks, work items)
