@@ -72,6 +72,12 @@ def lib():
             "bnb_get_tuning": (i, [p, p, p]),
             "bnb_autotune": (i, [p, p, p, p, i, p, p]),
             "bnb_nbdirect_noalloc": (i, [p, i, p, p, p, i, p, p, p, i, p, p]),
+            "bnb_mlp_linear_forward": (i, [i, i, i, p, p, p, i, p, p, p, p]),
+            "bnb_mlp_linear_backward": (i, [i, i, i, p, p, i, p, p, p, p, p, p, p, p]),
+            "bnb_mlp_mse": (i, [i, i, p, p, p, p, p, p]),
+            "bnb_mlp_adam": (i, [i, p, p, p, p, p, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, i, p]),
+            "bnb_to_bf16": (i, [i, p, p, p]),
+            "bnb_lambda_histogram": (i, [i, p, p, i, p, p, p, p, p]),
             "bnb_bond_gradient": (i, [i, p, p, p, p, p, p]),
             "bnb_langevin_vrorv": (i, [i, i, p, p, p, p, p, p, p, p, d, d, d, d, d, C.c_ulonglong, C.c_ulonglong,
                                        p, p, p, p]),

@@ -52,7 +52,8 @@ class MsldBatch:
     """State and step of R MSLD replicas on one GPU."""
 
     def __init__(self, reps: list[System], dt_fs: float = 2.0, T: float = 300.0, gamma_ps: float = 1.0,
-                 seed: int = 1, rebuild_every: int = 10, energy_every: int = 10, device="cuda", tune=False):
+                 seed: int = 1, rebuild_every: int = 10, energy_every: int = 10, device="cuda", tune=False,
+                 theta_mass: float = THETA_MASS, gamma_theta_ps: float | None = None):
         import torch
         self.torch = torch
         self.reps = reps
@@ -112,10 +113,10 @@ class MsldBatch:
         self.lambda_site = torch.from_numpy(np.concatenate(site).astype(np.int32)).to(self.dev)
         self.fixed = torch.from_numpy(np.concatenate(fixed).astype(np.uint8)).to(self.dev)
         self.fnex = reps[0].msld.fnex if reps[0].msld else 5.5
-        ism_t = np.full(L, 1 / math.sqrt(THETA_MASS))
+        ism_t = np.full(L, 1 / math.sqrt(theta_mass))
         ism_t[np.concatenate(fixed).astype(bool)] = np.inf  # frozen, as fixed blocks in the reference
         self.ismt = torch.from_numpy(ism_t).to(self.dev)
-        self.vt = torch.from_numpy(rng.normal(size=L) * math.sqrt(kT / THETA_MASS)).to(self.dev)
+        self.vt = torch.from_numpy(rng.normal(size=L) * math.sqrt(kT / theta_mass)).to(self.dev)
         self.vt[self.fixed.bool()] = 0
         self.lam = torch.zeros(L, dtype=f64, device=self.dev)
         self.lamf = torch.zeros(L, dtype=f32, device=self.dev)
@@ -129,7 +130,13 @@ class MsldBatch:
         a = math.exp(-gamma_ps / PICOSECOND * self.dt)
         self.fric = a
         self.noise = math.sqrt((1 - a * a) * kT)
+        at = a if gamma_theta_ps is None else math.exp(-gamma_theta_ps / PICOSECOND * self.dt)
+        self.fric_t = at                                  # theta friction (Msld gamma, msld.cu:46, 232-235)
+        self.noise_t = math.sqrt((1 - at * at) * kT)
         self._lambda_from_theta()
+        self.fixed_bias = None                             # lambda biases (set_bias)
+        self.var_bias = None
+        self.hist1 = None                                  # lambda histograms (enable_histograms)
         self.nb.update_domdec(self.xf, True)               # synchronous first build sizes the list
         if tune:
             self.tuned_ms = self.autotune()
@@ -154,15 +161,63 @@ class MsldBatch:
         if self.bond_start is not None:
             _lib.call("bnb_bond_gradient", self.nb.N, _p(self.bond_start), _p(self.bond_partner),
                       _p(self.bond_param), _p(self.x), _p(self.force), s)
+        if self.fixed_bias is not None:
+            _lib.call("bnb_bias", self.theta.numel(), _p(self.lam), _p(self.fixed_bias), self.n_var,
+                      _p(self.var_bias), _p(self.lforce), None, s)
         self.tforce.zero_()
         _lib.call("bnb_theta_force", self.lambda_site.numel(), _p(self.lambda_site), _p(self.site_bound),
                   float(self.fnex), _p(self.lam), _p(self.theta), _p(self.lforce), _p(self.fixed), _p(self.tforce), s)
         _lib.call("bnb_langevin_vrorv", self.x.numel(), self.theta.numel(), _p(self.x), _p(self.v), _p(self.force),
                   _p(self.ismx), _p(self.theta), _p(self.vt), _p(self.tforce), _p(self.ismt), self.dt, self.fric,
-                  self.noise, self.fric, self.noise, C.c_ulonglong(self.seed), C.c_ulonglong(0),
+                  self.noise, self.fric_t, self.noise_t, C.c_ulonglong(self.seed), C.c_ulonglong(0),
                   _p(self.step_counter), _p(self.xf), _p(self.nan), s)
         _lib.call("bnb_lambda_from_theta", self.site_bound.numel() - 1, _p(self.site_bound), float(self.fnex),
                   _p(self.theta), _p(self.fixed), _p(self.lam), _p(self.lamf), s)
+        if self.hist1 is not None:
+            _lib.call("bnb_lambda_histogram", self.theta.numel(), _p(self.lam), _p(self.fixed), self.n_pairs,
+                      _p(self.hist_pairs), _p(self.hist1), _p(self.hist2), _p(self.hist_end), s)
+
+    # -- lambda biases and histograms (adaptive landscape flattening) -------------
+    def set_bias(self, fixed: np.ndarray, var: np.ndarray):
+        """Fixed bias per global block (FP64 [L]) and variable biases
+        (``msld.VARBIAS_DTYPE``, global block indices).  Updating biases of
+        the same count rewrites the captured buffers in place, so a recorded
+        graph picks them up."""
+        torch = self.torch
+        fixed_t = torch.from_numpy(np.ascontiguousarray(fixed, np.float64))
+        var_t = torch.from_numpy(np.ascontiguousarray(var).view(np.uint8).copy())
+        if self.fixed_bias is not None and self.var_bias.numel() == var_t.numel():
+            self.fixed_bias.copy_(fixed_t)
+            self.var_bias.copy_(var_t)
+            return
+        self.graph = None
+        self.fixed_bias = fixed_t.to(self.dev)
+        self.var_bias = var_t.to(self.dev)
+        self.n_var = len(var)
+
+    def enable_histograms(self, pairs: np.ndarray):
+        """Sample lambda into histograms after every step (bnb_lambda_histogram);
+        ``pairs`` [P,2] global block pairs for the 8x8 histograms."""
+        torch = self.torch
+        L = self.theta.numel()
+        self.n_pairs = len(pairs)
+        self.hist_pairs = torch.from_numpy(np.ascontiguousarray(pairs, np.int32).reshape(-1)).to(self.dev)
+        self.hist1 = torch.zeros(L * 32, dtype=torch.int32, device=self.dev)
+        self.hist2 = torch.zeros(max(1, self.n_pairs) * 64, dtype=torch.int32, device=self.dev)
+        self.hist_end = torch.zeros(L, dtype=torch.int32, device=self.dev)
+        self.graph = None
+
+    def take_histograms(self):
+        """(hist1 [L,32], hist2 [P,8,8], endCount [L]) as numpy, then cleared.
+        The samples taken are the row sums of hist1 (one count per step)."""
+        L = self.theta.numel()
+        h1 = self.hist1.cpu().numpy().reshape(L, 32).astype(np.int64)
+        h2 = self.hist2.cpu().numpy()[:64 * self.n_pairs].reshape(self.n_pairs, 8, 8).astype(np.int64)
+        he = self.hist_end.cpu().numpy().astype(np.int64)
+        self.hist1.zero_()
+        self.hist2.zero_()
+        self.hist_end.zero_()
+        return h1, h2, he
 
     def run_eager(self, nsteps: int):
         for k in range(nsteps):

@@ -107,6 +107,31 @@ __global__ void k_bias(int blockCount, const L *lambda, const L *fixedBias, int 
   if (energy) warp_energy(e, energy);
 }
 
+// Lambda histograms of one sampling step (the data ALF builds from the .lmd
+// lambda trajectory that Msld writes every freqLMD steps, src/io/io.cxx:347-371):
+// per block a 32-bin histogram of lambda on [0,1] and a count of lambda > 0.99
+// (the block's end state); per listed block pair an 8x8 histogram of
+// (lambda_i, lambda_j).  Fixed blocks are skipped.
+__global__ void k_lambda_histogram(int blockCount, const double *lambda, const uint8_t *fixed, int pairCount,
+                                   const int *pairs, unsigned int *hist1, unsigned int *hist2,
+                                   unsigned int *endCount) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < blockCount && !(fixed && fixed[t])) {
+    const double l = lambda[t];
+    int b = (int)(l * 32.0);
+    b = b < 0 ? 0 : (b > 31 ? 31 : b);
+    if (hist1) atomicAdd(&hist1[32 * t + b], 1u);
+    if (endCount && l > 0.99) atomicAdd(&endCount[t], 1u);
+  }
+  if (t < pairCount && hist2) {
+    const double li = lambda[pairs[2 * t]], lj = lambda[pairs[2 * t + 1]];
+    int a = (int)(li * 8.0), b = (int)(lj * 8.0);
+    a = a < 0 ? 0 : (a > 7 ? 7 : a);
+    b = b < 0 ? 0 : (b > 7 ? 7 : b);
+    atomicAdd(&hist2[64 * t + 8 * a + b], 1u);
+  }
+}
+
 inline int blocks_for(int n) { return n > 0 ? (n + 255) / 256 : 1; }
 
 template <typename L, typename F>
@@ -168,4 +193,16 @@ extern "C" int bnb_bias(int blockCount, const double *lambda, const double *fixe
 extern "C" int bnb_bias_f32(int blockCount, const float *lambda, const float *fixedBias, int varCount,
                             const bnb_varbias *varBias, float *lambdaForce, double *energy, void *stream) {
   return bias<float, float>(blockCount, lambda, fixedBias, varCount, varBias, lambdaForce, energy, stream);
+}
+
+extern "C" int bnb_lambda_histogram(int blockCount, const double *lambda, const uint8_t *blockFixed,
+                                    int pairCount, const int *pairs, unsigned int *hist1, unsigned int *hist2,
+                                    unsigned int *endCount, void *stream) {
+  if (blockCount < 0 || pairCount < 0 || (blockCount > 0 && !lambda) || (pairCount > 0 && !pairs))
+    return BNB_ERR_ARG;
+  const int n = blockCount > pairCount ? blockCount : pairCount;
+  if (n == 0) return BNB_OK;
+  k_lambda_histogram<<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(blockCount, lambda, blockFixed, pairCount,
+                                                                      pairs, hist1, hist2, endCount);
+  return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
 }

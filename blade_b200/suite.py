@@ -2,7 +2,8 @@
 
     python -m blade_b200.suite msld   [--steps K]   # MSLD water box: pairs/s, parity, reference CUDA
     python -m blade_b200.suite batch  [--replicas R --steps K]   # batched vs one-at-a-time ns/day
-    python -m blade_b200.suite alf    [...]         # learned vs plain flattening (see blade_b200.alf)
+    python -m blade_b200.suite alf    [--replicas R --steps K --iters T --rounds n --eval-iters E]
+                                                    # learned vs plain flattening (blade_b200.alf)
 
 ``bench.py`` carries the headline metric (the 23,558-atom system); this module
 covers the other rows of the same metric.  Timings are device time from CUDA
@@ -165,6 +166,85 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def _gen_flat(seed):
+    from . import alf
+    return alf.flattening_system(seed)
+
+
+def flattening_replicas(seeds, workers=None):
+    workers = workers or min(16, os.cpu_count() or 1)
+    with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(_gen_flat, list(seeds)))
+
+
+def run_alf(args):
+    """Learned vs plain flattening: plain runs on seeded training systems give
+    (histogram, lookahead change) pairs; the BF16 MLP is trained on them with
+    libbnb's kernels; both methods then run on held-out systems, batched."""
+    import torch
+    from . import alf
+    t0 = time.time()
+    R, K = args.replicas, args.steps
+    Xs, Ys, Xv, Yv, rounds = [], [], [], [], []
+    for rnd in range(args.rounds):
+        reps = flattening_replicas(range(10000 + 1000 * rnd, 10000 + 1000 * rnd + R))
+        drv = alf.AlfBatch(reps, steps=K, seed=11 + rnd)
+        a, b = _events()
+        a.record()
+        recs = alf.run_sites(drv, args.iters)
+        b.record()
+        torch.cuda.synchronize()
+        st = drv.status()
+        drv.close()
+        X, Y = alf.training_pairs(drv.sm, recs)
+        rep = np.tile(np.arange(R), len(X) // R)
+        val = rep >= int(0.9 * R)                       # last 10 % of the replicas: validation
+        Xs.append(X[~val]); Ys.append(Y[~val]); Xv.append(X[val]); Yv.append(Y[val])
+        itf = alf.site_iterations_to_flat([(r["site_dev"], r["site_frac"]) for r in recs])
+        rounds.append({"seconds_gpu": a.elapsed_time(b) / 1e3, "status": st, "sites_flat": float((itf > 0).mean())})
+        print(json.dumps({"round": rnd, **rounds[-1], "pairs": len(X), "t": time.time() - t0}), file=sys.stderr,
+              flush=True)
+    X, Y, X_val, Y_val = (np.concatenate(a) for a in (Xs, Ys, Xv, Yv))
+    model = alf.new_model(seed=0)
+    a, b = _events()
+    a.record()
+    first, last, val = alf.train(model, X, Y, steps=args.train_steps, X_val=X_val, Y_val=Y_val,
+                                 log=lambda st, l: print(f"train {st} {l:.5f}", file=sys.stderr, flush=True))
+    b.record()
+    torch.cuda.synchronize()
+    t_train = a.elapsed_time(b) / 1e3
+    if args.save:
+        np.savez_compressed(args.save, **model.state())
+    # evaluation on held-out systems: same systems, same MD seed, both methods
+    reps = flattening_replicas(range(50000, 50000 + R))
+    out = {}
+    for name, mdl in (("plain", None), ("learned", model)):
+        drv = alf.AlfBatch(reps, steps=K, seed=99)
+        recs = alf.run_sites(drv, args.eval_iters, mdl)
+        st = drv.status()
+        drv.close()
+        itf = alf.site_iterations_to_flat([(r["site_dev"], r["site_frac"]) for r in recs])
+        capped = np.where(itf > 0, itf, args.eval_iters + 1)
+        fb = [float(r["fallback"].mean()) for r in recs if r["fallback"] is not None]
+        out[name] = {"median_iterations_to_flat": float(np.median(capped)), "mean_iterations_to_flat": float(capped.mean()),
+                     "sites_flat": float((itf > 0).mean()),
+                     "site_dev_median_per_iteration": [round(float(np.median(r["site_dev"])), 3) for r in recs],
+                     "fallback_fraction": float(np.mean(fb)) if fb else None, "status": st}
+    line = {"config": f"learned flattening: {R} batched replicas of the 216-water box + 3 sites x 4 substituents "
+                      f"(variants of one fragment), {K} steps (x 2 fs) per iteration",
+            "flat_criterion": f"per site: max |end-state population - 1/4| <= {alf.FLAT_TOL}, "
+                              f">= {alf.END_FRAC_MIN} of samples at end states",
+            "training": {"pairs": int(len(X)), "validation_pairs": int(len(X_val)), "rounds": rounds,
+                         "iterations_per_round": args.iters, "lookahead": alf.LOOKAHEAD,
+                         "mlp": [alf.FEAT_PAD, *alf.HIDDEN, alf.OUT_PAD], "steps": args.train_steps,
+                         "loss_first": first, "loss_last": last, "loss_validation": val, "seconds_gpu": t_train},
+            "eval_iterations": args.eval_iters, **out,
+            "ratio_learned_to_plain_median_iterations": out["learned"]["median_iterations_to_flat"]
+            / out["plain"]["median_iterations_to_flat"],
+            "seconds_total": time.time() - t0}
+    print(json.dumps(line), flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["msld", "batch", "alf"])
@@ -172,14 +252,18 @@ def main(argv=None):
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--tune-sequential", action="store_true")
+    ap.add_argument("--iters", type=int, default=60)
+    ap.add_argument("--rounds", type=int, default=3)
+    ap.add_argument("--eval-iters", type=int, default=30)
+    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--save", default=None)
     args, rest = ap.parse_known_args(argv)
     if args.what == "msld":
         run_msld(args)
     elif args.what == "batch":
         run_batch(args)
     else:
-        from . import alf
-        alf.main(rest)
+        run_alf(args)
 
 
 if __name__ == "__main__":

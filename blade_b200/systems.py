@@ -360,14 +360,17 @@ def _nearby(points: np.ndarray | None, center: np.ndarray, cut: float, box: floa
 
 
 def _add_sites(rng, fixed_atoms, anchors: np.ndarray, subs_per_site, box: float, dmin: float = 2.2,
-               avoid_sites: bool = True, outward: np.ndarray | None = None):
+               avoid_sites: bool = True, outward: np.ndarray | None = None, shared_geometry: bool = False):
     """Grow substituents at each anchor; returns atoms, per-atom (site, block), exclusions.
 
     Substituents of one site overlap each other (they are alternatives and
     mutually excluded); they keep ``dmin`` from ``fixed_atoms`` (the solute)
     and, with ``avoid_sites``, from the substituents of the other sites, with
     which they interact.  ``outward`` (unit vectors, one per site) moves the
-    walks' sphere 4 A off the anchor, away from the solute.
+    walks' sphere 4 A off the anchor, away from the solute.  With
+    ``shared_geometry`` the substituents of a site share one walk of 8-15
+    atoms (alchemical variants of one shape, differing in charges and LJ
+    types) instead of independent walks.
     """
     atoms, site_block, bonds_excl, site_members = [], [], [], []
     block = 1
@@ -382,14 +385,17 @@ def _add_sites(rng, fixed_atoms, anchors: np.ndarray, subs_per_site, box: float,
         near = [_nearby(fixed_atoms, center, 16.0, box)] + ([_nearby(other, center, 16.0, box)] if avoid_sites else [])
         near = [a for a in near if a is not None]
         avoid = np.concatenate(near) if near else None
+        template = None
         for _ in range(nsub):
-            n = int(rng.integers(8, 16))
-            start = anc + rng.normal(0, 0.3, 3) if out is None else anc + 2.0 * out + rng.normal(0, 0.3, 3)
-            for t in range(200):                       # a start point clear of the avoided atoms
-                if avoid is None or ((avoid - start) ** 2).sum(1).min() >= dmin * dmin:
-                    break
-                start = center + rng.normal(0, 0.6 + 0.02 * t, 3)
-            walk = chain_walk(rng, n, center, 6.0, start=start, avoid=avoid)
+            n = int(rng.integers(8, 16)) if template is None or not shared_geometry else len(template)
+            if template is None or not shared_geometry:
+                start = anc + rng.normal(0, 0.3, 3) if out is None else anc + 2.0 * out + rng.normal(0, 0.3, 3)
+                for t in range(200):                       # a start point clear of the avoided atoms
+                    if avoid is None or ((avoid - start) ** 2).sum(1).min() >= dmin * dmin:
+                        break
+                    start = center + rng.normal(0, 0.6 + 0.02 * t, 3)
+                template = chain_walk(rng, n, center, 6.0, start=start, avoid=avoid)
+            walk = template
             site_atoms.append(walk)
             idx = offset + np.arange(n)
             atoms.append(walk)
@@ -425,10 +431,29 @@ def _msld_layout(rng, subs_per_site, theta_range=(-math.pi / 2, math.pi / 2)) ->
     return Msld(nb, len(bound) - 1, bound, site, theta)
 
 
-def msld_water(seed: int = 3, sites: int = 3, subs: int = 4, clear: float = 2.2) -> System:
+def msld_water(seed: int = 3, sites: int = 3, subs: int = 4, clear: float = 2.2,
+               avoid_sites: bool = False, charge_sigma: float = 0.35, rigid_substituents: bool = False,
+               shared_geometry: bool = False, variant_sigma: float | None = None, variant_lj_atoms: int = 3,
+               tie_variants: bool = False) -> System:
     """Config-3 system: the water box plus MSLD sites anchored on water O's.
 
     Waters with any atom within ``clear`` A of a substituent are removed.
+    ``avoid_sites`` keeps substituents of different sites 2.2 A apart (for
+    dynamics; off by default so the seeded parity systems stay as they are).
+    ``charge_sigma`` is the spread of substituent charges (e).
+    ``rigid_substituents`` excludes every pair inside one substituent (a rigid
+    fragment: its internal energy does not change with lambda);
+    ``shared_geometry`` makes the substituents of a site variants of one shape;
+    with ``variant_sigma`` (needs ``shared_geometry``) they are also variants of
+    one fragment's parameters: the first substituent's charges plus
+    N(0, variant_sigma) e and its LJ types with ``variant_lj_atoms`` atoms
+    changed (eps x U(0.8,1.25), Rmin/2 x U(0.92,1.08)), as R-groups that
+    differ at a few atoms.  ``tie_variants`` (needs
+    ``shared_geometry``) adds zero-length bonds from every atom of a site's
+    first substituent to the same atom of the others, so that substituents
+    out of play (lambda ~ 0, hardly any nonbonded force) stay in place instead
+    of drifting through the solvent, as the unscaled bonded terms to the
+    common core hold them in a real MSLD system.
     """
     base = water_box(seed)
     rng = np.random.default_rng(seed + 1000)
@@ -443,7 +468,7 @@ def msld_water(seed: int = 3, sites: int = 3, subs: int = 4, clear: float = 2.2)
         if dd.min() >= 9.0:
             break
     subs_xyz, sb, sub_excl, nblock = _add_sites(rng, None, anchors, [subs] * sites, float(base.box[0]),
-                                                avoid_sites=False)
+                                                avoid_sites=avoid_sites, shared_geometry=shared_geometry)
     from scipy.spatial import cKDTree
     tree = cKDTree(np.mod(subs_xyz, base.box[0]), boxsize=float(base.box[0]))
     d, _ = tree.query(np.mod(base.xyz.astype(np.float64), base.box[0]), k=1)
@@ -454,7 +479,7 @@ def msld_water(seed: int = 3, sites: int = 3, subs: int = 4, clear: float = 2.2)
     xyz = np.concatenate([subs_xyz, wat]).astype(np.float32)
     N = len(xyz)
     nbd = np.zeros(N, NBOND_DTYPE)
-    q = rng.normal(0, 0.35, ns)
+    q = rng.normal(0, charge_sigma, ns)
     # each substituent neutral
     sbs = np.array(sb)
     for blk in np.unique(sbs[:, 1]):
@@ -464,14 +489,53 @@ def msld_water(seed: int = 3, sites: int = 3, subs: int = 4, clear: float = 2.2)
     nbd["siteBlock"][:ns] = (sbs[:, 0] << 16) | sbs[:, 1]
     nbd["q"][ns:] = np.tile(np.float32([TIP3P_Q_O, TIP3P_Q_H, TIP3P_Q_H]), len(keep))
     eps_s, rh_s = _lj_types(rng, ns)
+    if variant_sigma is not None and shared_geometry:
+        first = {}
+        for blk in np.unique(sbs[:, 1]):
+            m = np.nonzero(sbs[:, 1] == blk)[0]
+            site = int(sbs[m[0], 0])
+            if site not in first:
+                first[site] = m
+                continue
+            b0 = first[site]
+            dq = rng.normal(0, variant_sigma, len(m))
+            q[m] = q[b0] + dq - dq.mean()
+            eps_s[m], rh_s[m] = eps_s[b0], rh_s[b0]
+            redo = m[rng.choice(len(m), min(variant_lj_atoms, len(m)), replace=False)]
+            eps_s[redo] *= rng.uniform(0.8, 1.25, len(redo)).astype(np.float32)
+            rh_s[redo] *= rng.uniform(0.92, 1.08, len(redo)).astype(np.float32)
+        nbd["q"][:ns] = q.astype(np.float32)
     eps = np.concatenate([[TIP3P_EPS_H, TIP3P_EPS_O], eps_s])
     rh = np.concatenate([[TIP3P_RH_H, TIP3P_RH_O], rh_s])
     nbd["typeIdx"][:ns] = 2 + np.arange(ns)
     nbd["typeIdx"][ns:] = np.tile(np.int32([1, 0, 0]), len(keep))
     excl = np.concatenate([sub_excl, water_excl(ns, len(keep))])
+    sizes = np.bincount(sbs[:, 1])[1:]
+    if rigid_substituents:
+        intra = []
+        for f, n in zip(np.concatenate([[0], np.cumsum(sizes)[:-1]]), sizes):
+            a, b = np.meshgrid(np.arange(f, f + n), np.arange(f, f + n), indexing="ij")
+            keep_ab = a != b
+            intra.append(np.stack([a[keep_ab], b[keep_ab]], 1))
+        excl = np.unique(np.concatenate([excl] + intra).astype(np.int32), axis=0)
     msld = _msld_layout(rng, [subs] * sites)
+    firsts = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+    wb, wkb = water_bonds(ns, len(keep))
+    ties = []
+    if tie_variants and shared_geometry:
+        site_first = {}
+        for f, n, blk in zip(firsts, sizes, range(1, len(sizes) + 1)):
+            site = int(sbs[f, 0])
+            if site not in site_first:
+                site_first[site] = f
+            else:
+                f0 = site_first[site]
+                ties.append(np.stack([f0 + np.arange(n), f + np.arange(n)], 1))
+    bonds = np.concatenate([chain_bonds(f, n) for f, n in zip(firsts, sizes)] + ties + [wb]).astype(np.int32)
+    kb = np.concatenate([np.full(len(bonds) - len(wb), KB_CHAIN), wkb])
     return System(f"msld_water_{N}", xyz, base.box.copy(), nbd, vdw_table(eps, rh), excl,
-                  base.rCut, base.rSwitch, base.betaEwald, msld=msld)
+                  base.rCut, base.rSwitch, base.betaEwald, msld=msld, bonds=bonds,
+                  bond_param=with_bond_lengths(xyz, bonds, kb))
 
 
 def msld_chain(seed: int, n_atoms: int, n_sites: int, subs_per_site, rCut=12.0, rSwitch=10.0,

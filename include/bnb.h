@@ -289,6 +289,19 @@ int bnb_bias_f32(int blockCount, const float *lambda, const float *fixedBias,
 int bnb_set_tuning(bnb_handle *h, int tilesPerWork, int ctasPerSM);
 int bnb_get_tuning(bnb_handle *h, int *tilesPerWork, int *ctasPerSM);
 /*
+ * Adds one sampling step of lambda (FP64, [blockCount]) to histograms, the
+ * statistics adaptive landscape flattening takes from the .lmd lambda
+ * trajectory (written by src/io/io.cxx:347-371): hist1[32*b + k] counts
+ * lambda_b in bin k of 32 on [0,1]; endCount[b] counts lambda_b > 0.99;
+ * hist2[64*p + 8*a + c] counts (lambda_i, lambda_j) of pair p =
+ * (pairs[2p], pairs[2p+1]) in the 8x8 bin (a, c).  Blocks with blockFixed
+ * set are skipped.  Any output may be NULL.  Counts are uint32.
+ */
+int bnb_lambda_histogram(int blockCount, const double *lambda, const uint8_t *blockFixed,
+                         int pairCount, const int *pairs, unsigned int *hist1,
+                         unsigned int *hist2, unsigned int *endCount, void *stream);
+
+/*
  * Autotuner: times every (tiles per work item in {4,8,16,32}) x (CTAs per SM
  * in {auto,2,3}) setting on the caller's coordinates (median of `reps`
  * evaluations, CUDA events), keeps the fastest and rebuilds the list with it.
@@ -329,6 +342,32 @@ int bnb_langevin_vrorv(int nx, int nt, double *x, double *v, const double *fx,
                        float *x_f, int *nanFlag, void *stream);
 
 /* Library version string. */
+/* ---- BF16 MLP of learned landscape flattening (no reference counterpart;
+ * BLaDE's src/mlp is TorchANI inference, unrelated).  Row-major arrays,
+ * BF16 as uint16_t bit patterns, products with BF16 operands and FP32
+ * accumulation in a fixed order.  act: 0 identity, 1 SiLU. ---------------- */
+/* Z[M,N] = X[M,K] W[N,K]^T + bias[N] (FP32, bias may be NULL); Y = act(Z)
+ * as BF16 [M,N] and/or FP32 Yf [M,N] (either may be NULL). */
+int bnb_mlp_linear_forward(int M, int N, int K, const uint16_t *X, const uint16_t *W,
+                           const float *bias, int act, float *Z, uint16_t *Y, float *Yf,
+                           void *stream);
+/* Given dY = dLoss/dY [M,N] (FP32) and the forward's Z: dZ = dY act'(Z)
+ * (FP32 [M,N] and its BF16 copy dZb), dW[N,K] = dZb^T X, db[N] = sum_m dZ,
+ * and, when dX is not NULL, dX[M,K] = dZb W.  dW and db are overwritten. */
+int bnb_mlp_linear_backward(int M, int N, int K, const float *dY, const float *Z, int act,
+                            const uint16_t *X, const uint16_t *W, float *dZ, uint16_t *dZb,
+                            float *dX, float *dW, float *db, void *stream);
+/* loss = (1/M) sum_{m,n} w[n] (Y-T)^2 (w may be NULL: 1), dY = dloss/dY. */
+int bnb_mlp_mse(int M, int N, const float *Y, const float *T, const float *weight, float *dY,
+                double *loss, void *stream);
+/* Adam step (bias-corrected, decoupled weight decay) on FP32 master weights;
+ * writes the BF16 working copy when weightBf16 is not NULL.  step >= 1. */
+int bnb_mlp_adam(int n, float *master, uint16_t *weightBf16, const float *grad, float *m,
+                 float *v, float lr, float beta1, float beta2, float eps, float weightDecay,
+                 int step, void *stream);
+/* y = bf16(x), round to nearest even. */
+int bnb_to_bf16(int n, const float *x, uint16_t *y, void *stream);
+
 const char *bnb_version(void);
 
 #ifdef __cplusplus
