@@ -74,7 +74,7 @@ def lib():
             "bnb_nbdirect_noalloc": (i, [p, i, p, p, p, i, p, p, p, i, p, p]),
             "bnb_mlp_linear_forward": (i, [i, i, i, p, p, p, i, p, p, p, p]),
             "bnb_mlp_linear_backward": (i, [i, i, i, p, p, i, p, p, p, p, p, p, p, p]),
-            "bnb_mlp_mse": (i, [i, i, p, p, p, p, p, p]),
+            "bnb_mlp_mse": (i, [i, i, p, p, p, p, p, p, p]),
             "bnb_mlp_adam": (i, [i, p, p, p, p, p, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, i, p]),
             "bnb_to_bf16": (i, [i, p, p, p]),
             "bnb_lambda_histogram": (i, [i, p, p, i, p, p, p, p, p]),

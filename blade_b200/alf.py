@@ -438,13 +438,43 @@ def training_pairs(sm: SiteMap, recs, lookahead: int = LOOKAHEAD):
     return np.concatenate(X), np.concatenate(Y)
 
 
+def flat_targets(Xseq: np.ndarray):
+    """Targets that point at flatness: for features Xseq [T, R, FEAT_PAD] of
+    consecutive plain iterations of R replicas, each site's target is the
+    change from its current parameters to those it had at the first iteration
+    its histograms were flat (zero from then on); sites that never became
+    flat get weight 0.  Flatness is judged on the top histogram bin
+    (lambda > 31/32) standing in for the end-state count.  Returns
+    (Y, W) [T, R, OUT_PAD] with Y scaled by 1/TARGET_SCALE."""
+    T, R, _ = Xseq.shape
+    per = SITES * SUBS * 32 + SITES * N_PAIRS_SITE * 64
+    nps = n_site_params(SUBS)
+    Y = np.zeros((T, R, OUT_PAD), np.float32)
+    W = np.zeros((T, R, OUT_PAD), np.float32)
+    for s in range(SITES):
+        h = Xseq[:, :, s * SUBS * 32:(s + 1) * SUBS * 32].reshape(T, R, SUBS, 32).astype(np.float64)
+        end = h[..., 31]
+        tot = end.sum(-1)
+        p = end / np.maximum(tot, 1e-12)[..., None]
+        flat = (np.abs(p - 1.0 / SUBS).max(-1) <= FLAT_TOL) & (tot >= END_FRAC_MIN)
+        q = Xseq[:, :, per + s * nps:per + (s + 1) * nps].astype(np.float64) * PARAM_SCALE
+        for r in range(R):
+            hit = np.nonzero(flat[:, r])[0]
+            if len(hit) == 0:
+                continue
+            t0 = hit[0]
+            Y[:t0, r, s * nps:(s + 1) * nps] = (q[t0, r] - q[:t0, r]) / TARGET_SCALE
+            W[:, r, s * nps:(s + 1) * nps] = 1.0
+    return Y, W
+
+
 def new_model(seed: int = 0, max_batch: int = 256):
     from .mlp import BF16MLP
     return BF16MLP([FEAT_PAD, *HIDDEN, OUT_PAD], max_batch=max_batch, seed=seed)
 
 
 def train(model, X, Y, steps: int = 3000, batch: int = 256, lr: float = 1e-3, seed: int = 0, n_aug: int = 64,
-          X_val=None, Y_val=None, log=None):
+          X_val=None, Y_val=None, log=None, W=None, W_val=None):
     """Adam on the MSE, every step on a batch relabeled by a random site /
     substituent permutation (the task is symmetric under relabeling).
     Returns (first loss, last loss, validation loss or None)."""
@@ -460,21 +490,27 @@ def train(model, X, Y, steps: int = 3000, batch: int = 256, lr: float = 1e-3, se
         xb = X[idx][:, fmap]
         yb = Y[idx].copy()
         yb[:, :N_PARAMS_REP] = yb[:, :N_PARAMS_REP][:, qmap]
+        wb = None
+        if W is not None:
+            wb = W[idx].copy()
+            wb[:, :N_PARAMS_REP] = wb[:, :N_PARAMS_REP][:, qmap]
+            wb = torch.from_numpy(np.ascontiguousarray(wb)).to(dev)
         lr_t = lr * 0.5 * (1 + math.cos(math.pi * step / steps))
         loss = model.train_step(torch.from_numpy(np.ascontiguousarray(xb)).to(dev),
-                                torch.from_numpy(np.ascontiguousarray(yb)).to(dev), lr=lr_t)
+                                torch.from_numpy(np.ascontiguousarray(yb)).to(dev), lr=lr_t, elem_weight=wb)
         if step == 0:
             first = float(loss.cpu()[0])
         if log and step % 500 == 0:
             log(step, float(loss.cpu()[0]))
-    last = float(loss.cpu()[0])
+    last = float(loss.cpu()[0]) if steps else None
     val = None
     if X_val is not None and len(X_val):
         tot, cnt = 0.0, 0
         for k in range(0, len(X_val), model.max_batch):
             xb = torch.from_numpy(np.ascontiguousarray(X_val[k:k + model.max_batch])).to(dev)
             yb = torch.from_numpy(np.ascontiguousarray(Y_val[k:k + model.max_batch])).to(dev)
-            tot += float(model.loss_grad(xb, yb).cpu()[0]) * len(xb)
+            wb = None if W_val is None else torch.from_numpy(np.ascontiguousarray(W_val[k:k + model.max_batch])).to(dev)
+            tot += float(model.loss_grad(xb, yb, elem_weight=wb).cpu()[0]) * len(xb)
             cnt += len(xb)
         val = tot / cnt
     return first, last, val
@@ -491,10 +527,11 @@ def site_iterations_to_flat(recs_dev_frac) -> np.ndarray:
     return first
 
 
-def run_sites(drv: AlfBatch, n_iter: int, model=None):
+def run_sites(drv: AlfBatch, n_iter: int, model=None, scale: float = 1.0, with_plain: bool = False):
     """n_iter iterations of plain (model None) or learned flattening; returns
     per-iteration records with per-site flatness and whether the plain
-    fallback was used."""
+    fallback was used.  The learned step is ``scale`` times the predicted
+    lookahead change, added to the plain update when ``with_plain``."""
     import torch
     R = drv.sm.n_replicas
     prev = np.full(R, np.inf)
@@ -513,10 +550,51 @@ def run_sites(drv: AlfBatch, n_iter: int, model=None):
             X = torch.from_numpy(replica_features(drv.sm, h1, h2, drv.params)).to(drv.B.dev)
             pred = model.forward(X).cpu().numpy()[:, :N_PARAMS_REP].astype(np.float64) * TARGET_SCALE
             bad = ~np.isfinite(pred).all(1) | (used_learned & (rdev > prev + JUDGE_MARGIN))
-            delta = np.where(np.repeat(bad, N_PARAMS_REP), plain, pred.reshape(-1))
+            step = scale * pred.reshape(-1) + (plain if with_plain else 0.0)
+            delta = np.where(np.repeat(bad, N_PARAMS_REP), plain, step)
             used_learned = ~bad
             rec["fallback"] = bad
         prev = rdev
         recs.append(rec)
         drv.set_params(drv.params + delta)
     return recs
+
+
+def _replica_map() -> SiteMap:
+    """Site map of one replica of 3 sites x 4 substituents (blocks 1..12)."""
+    sites = [np.arange(1 + SUBS * k, 1 + SUBS * (k + 1)) for k in range(SITES)]
+    pairs = np.array([(g[a], g[b]) for g in sites for a in range(SUBS) for b in range(a + 1, SUBS)], np.int32)
+    return SiteMap(sites, np.zeros(SITES, np.int64), pairs, np.arange(SITES + 1) * N_PAIRS_SITE,
+                   np.arange(SITES + 1) * n_site_params(SUBS), 1, 1 + SITES * SUBS)
+
+
+def plain_update_from_features(x: np.ndarray, samples: int) -> np.ndarray:
+    """The plain update recomputed from one replica's features (histograms
+    times ``samples``; the top 1-D bin stands in for the end-state count)."""
+    sm = _replica_map()
+    h1 = np.zeros((sm.n_blocks, 32), np.int64)
+    h2 = np.zeros((len(sm.pairs), 8, 8), np.int64)
+    o2 = SITES * SUBS * 32
+    for k in range(SITES):
+        h1[1 + SUBS * k:1 + SUBS * (k + 1)] = np.round(x[k * SUBS * 32:(k + 1) * SUBS * 32].reshape(SUBS, 32)
+                                                       * samples)
+        h2[N_PAIRS_SITE * k:N_PAIRS_SITE * (k + 1)] = np.round(
+            x[o2 + k * N_PAIRS_SITE * 64:o2 + (k + 1) * N_PAIRS_SITE * 64].reshape(N_PAIRS_SITE, 8, 8) * samples)
+    return plain_update(sm, h1, h2, h1[:, 31].copy())
+
+
+def distance_to_flat(X: np.ndarray, Y: np.ndarray, W: np.ndarray, pred: np.ndarray, samples: int):
+    """RMS distance (kcal/mol, weighted entries only) from the flat parameters
+    of (a) the network's step, (b) the plain update, (c) no change."""
+    em, ep, e0 = [], [], []
+    for n in range(len(X)):
+        sel = W[n, :N_PARAMS_REP] > 0
+        if not sel.any():
+            continue
+        tgt = Y[n, :N_PARAMS_REP].astype(np.float64) * TARGET_SCALE
+        pu = plain_update_from_features(X[n].astype(np.float64), samples)
+        em.append(((pred[n, :N_PARAMS_REP] * TARGET_SCALE - tgt)[sel] ** 2).mean())
+        ep.append(((pu - tgt)[sel] ** 2).mean())
+        e0.append((tgt[sel] ** 2).mean())
+    return {"samples": len(em), "network": float(np.sqrt(np.mean(em))), "plain_update": float(np.sqrt(np.mean(ep))),
+            "no_change": float(np.sqrt(np.mean(e0)))}

@@ -6,7 +6,7 @@
 // trained and run with these kernels only:
 //   linear forward   Z = X W^T + b, Y = act(Z)  (X, W, Y in BF16; Z FP32)
 //   linear backward  dZ = dY act'(Z); dX = dZ W; dW = dZ^T X; db = sum_m dZ
-//   MSE loss         L = (1/M) sum_m sum_n w_n (Y - T)^2, dY = dL/dY
+//   MSE loss         L = (1/M) sum_m sum_n w_n w_mn (Y - T)^2, dY = dL/dY
 //   Adam             FP32 master weights, BF16 working copy
 // Every product takes BF16 operands (round to nearest even) and accumulates
 // in FP32 in a fixed order, so results are reproducible run to run.  act is
@@ -105,12 +105,13 @@ __global__ void k_colsum(int M, int N, const float *dZ, float *db) {
 }
 
 // One CTA: loss and dY of the weighted mean squared error, summed in a fixed order.
-__global__ void k_mse(int M, int N, const float *Y, const float *T, const float *w, float *dY, double *loss) {
+__global__ void k_mse(int M, int N, const float *Y, const float *T, const float *w, const float *we, float *dY,
+                      double *loss) {
   __shared__ double red[1024];
   double s = 0.0;
   const float inv = 1.f / (float)M;
   for (int t = threadIdx.x; t < M * N; t += blockDim.x) {
-    const float wn = w ? w[t % N] : 1.f;
+    const float wn = (w ? w[t % N] : 1.f) * (we ? we[t] : 1.f);
     const float d = Y[t] - T[t];
     dY[t] = 2.f * wn * d * inv;
     s += (double)wn * d * d;
@@ -186,10 +187,10 @@ extern "C" int bnb_mlp_linear_backward(int M, int N, int K, const float *dY, con
   return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
 }
 
-extern "C" int bnb_mlp_mse(int M, int N, const float *Y, const float *T, const float *weight, float *dY,
-                           double *loss, void *stream) {
+extern "C" int bnb_mlp_mse(int M, int N, const float *Y, const float *T, const float *weight,
+                           const float *elemWeight, float *dY, double *loss, void *stream) {
   if (M <= 0 || N <= 0 || !Y || !T || !dY) return BNB_ERR_ARG;
-  k_mse<<<1, 1024, 0, (cudaStream_t)stream>>>(M, N, Y, T, weight, dY, loss);
+  k_mse<<<1, 1024, 0, (cudaStream_t)stream>>>(M, N, Y, T, weight, elemWeight, dY, loss);
   return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
 }
 

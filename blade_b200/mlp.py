@@ -91,13 +91,15 @@ class BF16MLP:
                       _p(self.gb[l]), s)
             dy = dx
 
-    def loss_grad(self, x, target, weight=None):
-        """Forward + MSE + backward; returns the device loss tensor (FP64 [1])."""
+    def loss_grad(self, x, target, weight=None, elem_weight=None):
+        """Forward + MSE + backward; returns the device loss tensor (FP64 [1]).
+        weight: per output column [N]; elem_weight: per element [M, N]."""
         M = x.shape[0]
         out = self.forward(x)
         dout = self.dY[-1]
-        _lib.call("bnb_mlp_mse", M, self.sizes[-1], _p(out), _p(target.contiguous()), _p(weight), _p(dout),
-                  _p(self.loss), self._s())
+        ew = None if elem_weight is None else elem_weight.contiguous()
+        _lib.call("bnb_mlp_mse", M, self.sizes[-1], _p(out), _p(target.contiguous()), _p(weight), _p(ew),
+                  _p(dout), _p(self.loss), self._s())
         self.backward(M, dout)
         return self.loss
 
@@ -110,8 +112,8 @@ class BF16MLP:
             _lib.call("bnb_mlp_adam", self.b[l].numel(), _p(self.b[l]), None, _p(self.gb[l]), _p(self.mb[l]),
                       _p(self.vb[l]), lr, beta1, beta2, eps, 0.0, self.step_count, s)
 
-    def train_step(self, x, target, weight=None, lr=1e-3):
-        loss = self.loss_grad(x, target, weight)
+    def train_step(self, x, target, weight=None, lr=1e-3, elem_weight=None):
+        loss = self.loss_grad(x, target, weight, elem_weight)
         self.adam_step(lr)
         return loss
 

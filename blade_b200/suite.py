@@ -1,5 +1,6 @@
 """Measurements of the MSLD and batched configurations (one JSON line each).
 
+    python -m blade_b200.suite water  [--steps K]   # 216-water box: pairs/s, parity, reference CUDA
     python -m blade_b200.suite msld   [--steps K]   # MSLD water box: pairs/s, parity, reference CUDA
     python -m blade_b200.suite batch  [--replicas R --steps K]   # batched vs one-at-a-time ns/day
     python -m blade_b200.suite alf    [--replicas R --steps K --iters T --rounds n --eval-iters E]
@@ -49,12 +50,15 @@ def _events():
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
-def run_msld(args):
+def run_msld(args, water_only=False):
+    """One system, many evaluations: pairs/s, error against the FP64 oracle,
+    and the reference's CUDA build on the same GPU.  water_only: the 216-water
+    box without MSLD sites, else the MSLD box."""
     import torch
     import oracle
     from oracle import refgpu
     from .nbdirect import NbDirect
-    s = systems.msld_water()
+    s = systems.water_box() if water_only else systems.msld_water()
     nb = NbDirect(s)
     pos = nb.positions_tensor()
     lam = nb.lambdas_tensor()
@@ -67,7 +71,9 @@ def run_msld(args):
     g = f64.cpu().numpy()
     ferr = float(np.sqrt(((g - o["grad"]) ** 2).sum() / (o["grad"] ** 2).sum()))
     lf = l64.cpu().numpy()
-    lerr = float(np.sqrt(((lf[1:] - o["lambdaForce"][1:]) ** 2).sum() / (o["lambdaForce"][1:] ** 2).sum()))
+    lerr = (float(np.sqrt(((lf[1:] - o["lambdaForce"][1:]) ** 2).sum() / (o["lambdaForce"][1:] ** 2).sum()))
+            if s.msld else None)
+    e_rel = float(abs(float(e64.cpu()[0]) - o["energy"]) / abs(o["energy"]))
     K = args.steps
     force = torch.zeros(3 * s.N, device="cuda")
     lforce = torch.zeros(nb.L, device="cuda")
@@ -82,17 +88,18 @@ def run_msld(args):
     b.record()
     torch.cuda.synchronize()
     t = a.elapsed_time(b) / 1e3
-    line = {"config": "msld_water (216-water box + 3 sites x 4 substituents, soft core)", "atoms": s.N,
-            "lambda_blocks": s.msld.blockCount, "pairs_per_eval": pairs, "pairs_oracle": o["pairs"],
-            "force_rel_rms_vs_fp64": ferr, "dUdlambda_rel_rms_vs_fp64": lerr,
+    line = {"config": ("water_box (216 TIP3P, 18.856 A, rc 9 / rs 8, beta 0.34)" if water_only else
+                       "msld_water (216-water box + 3 sites x 4 substituents, soft core)"), "atoms": s.N,
+            "lambda_blocks": s.msld.blockCount if s.msld else 1, "pairs_per_eval": pairs, "pairs_oracle": o["pairs"],
+            "force_rel_rms_vs_fp64": ferr, "dUdlambda_rel_rms_vs_fp64": lerr, "energy_rel_err_vs_fp64": e_rel,
             "bnb": {"pairs_per_s": pairs * K / t, "ms_per_step": 1e3 * t / K}}
     if refgpu.available():
         ref = refgpu.RefGPU(s)
         r = ref.evaluate()
         line["reference_vs_fp64"] = {
             "force_rel_rms": float(np.sqrt(((r["grad"] - o["grad"]) ** 2).sum() / (o["grad"] ** 2).sum())),
-            "dUdlambda_rel_rms": float(np.sqrt(((r["lambdaForce"][1:] - o["lambdaForce"][1:]) ** 2).sum()
-                                               / (o["lambdaForce"][1:] ** 2).sum()))}
+            "dUdlambda_rel_rms": (float(np.sqrt(((r["lambdaForce"][1:] - o["lambdaForce"][1:]) ** 2).sum()
+                                                / (o["lambdaForce"][1:] ** 2).sum())) if s.msld else None)}
         frames = pos.double().repeat(K, 1)
         ref.time(frames[:10], 10, 10, 10)
         t_ref = ref.time(frames, K, 10, 10) / 1e3
@@ -122,6 +129,22 @@ def run_batch(args):
     torch.cuda.synchronize()
     t_batch = a.elapsed_time(b) / 1e3
     st, nan = B.check()
+    # where a batched step's time goes: 20 eager steps with the pair kernel and
+    # list rebuilds bracketed by CUDA events, and the in-cutoff pairs of one step
+    B.nb.profile(True)
+    a.record()
+    B.run_eager(20)
+    b.record()
+    torch.cuda.synchronize()
+    prof = B.nb.profile_read()
+    B.nb.profile(False)
+    B.nb.set_counting(True)
+    B.enqueue_step(0)                     # an energy step: the pair counter runs in the energy kernels
+    pairs = B.nb.pair_count()
+    B.nb.set_counting(False)
+    breakdown = {"eager_ms_per_step": a.elapsed_time(b) / 20, "pair_ms_per_step": prof["pair_ms"] / 20,
+                 "rebuild_ms_per_rebuild": prof["rebuild_ms"] / max(1, prof["rebuilds"]),
+                 "pairs_per_step": pairs, "pair_kernel_pairs_per_s": pairs / (prof["pair_ms"] / 20 / 1e3)}
     B.close()
     del B
     torch.cuda.empty_cache()
@@ -156,7 +179,7 @@ def run_batch(args):
             "steps": K, "step": "rebuild/10 + nbdirect(MSLD) + dU/dlambda->dU/dtheta + Langevin VRORV(x, theta) "
                                 "+ harmonic bonds + theta->lambda; no PME recip, angles, dihedrals or SHAKE",
             "batched_graph": {"seconds": t_batch, "ns_per_day_aggregate": ns_per_day(K, t_batch, replicas=R),
-                              "tuning": tuning, "status": st, "nan": nan},
+                              "tuning": tuning, "status": st, "nan": nan, "breakdown": breakdown},
             "sequential_eager": {"seconds": t_seq, "ns_per_day_aggregate": ns_per_day(K, t_seq, replicas=R)},
             "sequential_graph": {"seconds": t_seq_graph,
                                  "ns_per_day_aggregate": ns_per_day(K, t_seq_graph, replicas=R)},
@@ -186,7 +209,14 @@ def run_alf(args):
     t0 = time.time()
     R, K = args.replicas, args.steps
     Xs, Ys, Xv, Yv, rounds = [], [], [], [], []
-    for rnd in range(args.rounds):
+    if args.data_in:                                    # pairs made by an earlier "--data-out" run
+        for f in sorted(os.listdir(args.data_in)):
+            if f.startswith("alf_pairs_") and f.endswith(".npz"):
+                d = np.load(os.path.join(args.data_in, f))
+                Xs.append(d["X"].astype(np.float32)); Ys.append(d["Y"].astype(np.float32))
+                Xv.append(d["Xv"].astype(np.float32)); Yv.append(d["Yv"].astype(np.float32))
+                rounds.append(json.loads(str(d["meta"])))
+    for rnd in range(0 if args.data_in else args.rounds):
         reps = flattening_replicas(range(10000 + 1000 * rnd, 10000 + 1000 * rnd + R))
         drv = alf.AlfBatch(reps, steps=K, seed=11 + rnd)
         a, b = _events()
@@ -204,23 +234,58 @@ def run_alf(args):
         rounds.append({"seconds_gpu": a.elapsed_time(b) / 1e3, "status": st, "sites_flat": float((itf > 0).mean())})
         print(json.dumps({"round": rnd, **rounds[-1], "pairs": len(X), "t": time.time() - t0}), file=sys.stderr,
               flush=True)
+        if args.data_out:
+            os.makedirs(args.data_out, exist_ok=True)
+            np.savez_compressed(os.path.join(args.data_out, f"alf_pairs_{rnd}.npz"), X=Xs[-1].astype(np.float16),
+                                Y=Ys[-1], Xv=Xv[-1].astype(np.float16), Yv=Yv[-1], meta=json.dumps(rounds[-1]))
+    if args.data_out:
+        print(json.dumps({"pairs": int(sum(len(x) for x in Xs)), "rounds": rounds}), flush=True)
+        return
+    W = W_val = None
+    if args.target == "flat":                           # point at each site's first flat parameters
+        T_eff = args.iters - alf.LOOKAHEAD
+        R_val = R - int(0.9 * R)
+        Ys, Ws, Yv, Wv = [], [], [], []
+        for k in range(len(Xs)):
+            for src, dstY, dstW, n in ((Xs[k], Ys, Ws, R - R_val), (Xv[k], Yv, Wv, R_val)):
+                y, w = alf.flat_targets(src.reshape(T_eff, n, -1))
+                dstY.append(y.reshape(T_eff * n, -1))
+                dstW.append(w.reshape(T_eff * n, -1))
+        W, W_val = np.concatenate(Ws), np.concatenate(Wv)
     X, Y, X_val, Y_val = (np.concatenate(a) for a in (Xs, Ys, Xv, Yv))
     model = alf.new_model(seed=0)
     a, b = _events()
-    a.record()
-    first, last, val = alf.train(model, X, Y, steps=args.train_steps, X_val=X_val, Y_val=Y_val,
-                                 log=lambda st, l: print(f"train {st} {l:.5f}", file=sys.stderr, flush=True))
-    b.record()
-    torch.cuda.synchronize()
-    t_train = a.elapsed_time(b) / 1e3
+    if args.model_in:                                   # weights of an earlier training run
+        model.load(dict(np.load(args.model_in)))
+        first = last = None
+        val = alf.train(model, X[:0], Y[:0], steps=0, X_val=X_val, Y_val=Y_val, W_val=W_val)[2]
+        t_train = 0.0
+    else:
+        a.record()
+        first, last, val = alf.train(model, X, Y, steps=args.train_steps, X_val=X_val, Y_val=Y_val, W=W,
+                                     W_val=W_val,
+                                     log=lambda st, l: print(f"train {st} {l:.5f}", file=sys.stderr, flush=True))
+        b.record()
+        torch.cuda.synchronize()
+        t_train = a.elapsed_time(b) / 1e3
     if args.save:
         np.savez_compressed(args.save, **model.state())
+    offline = None
+    if W_val is not None:                               # one step toward the flat parameters, held-out data
+        preds = []
+        for k in range(0, len(X_val), model.max_batch):
+            xb = torch.from_numpy(np.ascontiguousarray(X_val[k:k + model.max_batch])).to(model.dev)
+            preds.append(model.forward(xb).cpu().numpy())
+        offline = alf.distance_to_flat(X_val, Y_val, W_val, np.concatenate(preds), K)
     # evaluation on held-out systems: same systems, same MD seed, both methods
     reps = flattening_replicas(range(50000, 50000 + R))
     out = {}
-    for name, mdl in (("plain", None), ("learned", model)):
+    modes = [m for m in args.eval_modes.split(",") if m]
+    for name in modes:                                  # plain | learned:<scale> | plain+learned:<scale>
+        mdl = None if name == "plain" else model
+        scale = float(name.split(":")[1]) if ":" in name else 1.0
         drv = alf.AlfBatch(reps, steps=K, seed=99)
-        recs = alf.run_sites(drv, args.eval_iters, mdl)
+        recs = alf.run_sites(drv, args.eval_iters, mdl, scale=scale, with_plain=name.startswith("plain+"))
         st = drv.status()
         drv.close()
         itf = alf.site_iterations_to_flat([(r["site_dev"], r["site_frac"]) for r in recs])
@@ -238,16 +303,15 @@ def run_alf(args):
                          "iterations_per_round": args.iters, "lookahead": alf.LOOKAHEAD,
                          "mlp": [alf.FEAT_PAD, *alf.HIDDEN, alf.OUT_PAD], "steps": args.train_steps,
                          "loss_first": first, "loss_last": last, "loss_validation": val, "seconds_gpu": t_train},
+            "step_distance_to_flat_parameters": offline,
             "eval_iterations": args.eval_iters, **out,
-            "ratio_learned_to_plain_median_iterations": out["learned"]["median_iterations_to_flat"]
-            / out["plain"]["median_iterations_to_flat"],
             "seconds_total": time.time() - t0}
     print(json.dumps(line), flush=True)
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["msld", "batch", "alf"])
+    ap.add_argument("what", choices=["water", "msld", "batch", "alf"])
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--seed", type=int, default=4)
@@ -257,9 +321,14 @@ def main(argv=None):
     ap.add_argument("--eval-iters", type=int, default=30)
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--save", default=None)
+    ap.add_argument("--data-out", default=None)
+    ap.add_argument("--data-in", default=None)
+    ap.add_argument("--model-in", default=None)
+    ap.add_argument("--eval-modes", default="plain,learned:1")
+    ap.add_argument("--target", default="flat", choices=["flat", "lookahead"])
     args, rest = ap.parse_known_args(argv)
-    if args.what == "msld":
-        run_msld(args)
+    if args.what in ("msld", "water"):
+        run_msld(args, water_only=args.what == "water")
     elif args.what == "batch":
         run_batch(args)
     else:

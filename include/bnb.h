@@ -357,9 +357,10 @@ int bnb_mlp_linear_forward(int M, int N, int K, const uint16_t *X, const uint16_
 int bnb_mlp_linear_backward(int M, int N, int K, const float *dY, const float *Z, int act,
                             const uint16_t *X, const uint16_t *W, float *dZ, uint16_t *dZb,
                             float *dX, float *dW, float *db, void *stream);
-/* loss = (1/M) sum_{m,n} w[n] (Y-T)^2 (w may be NULL: 1), dY = dloss/dY. */
-int bnb_mlp_mse(int M, int N, const float *Y, const float *T, const float *weight, float *dY,
-                double *loss, void *stream);
+/* loss = (1/M) sum_{m,n} w[n] we[m,n] (Y-T)^2, dY = dloss/dY; the column
+ * weights w [N] and element weights we [M,N] may each be NULL (all 1). */
+int bnb_mlp_mse(int M, int N, const float *Y, const float *T, const float *weight,
+                const float *elemWeight, float *dY, double *loss, void *stream);
 /* Adam step (bias-corrected, decoupled weight decay) on FP32 master weights;
  * writes the BF16 working copy when weightBf16 is not NULL.  step >= 1. */
 int bnb_mlp_adam(int n, float *master, uint16_t *weightBf16, const float *grad, float *m,

@@ -59,9 +59,11 @@ def linear_backward(dY, Z, act: int, X, W):
     return dZ, dZb, dZb @ W, dZb.T @ X, dZ.sum(0)
 
 
-def mse(Y, T, w=None):
+def mse(Y, T, w=None, we=None):
     M = Y.shape[0]
     w = np.ones(Y.shape[1]) if w is None else w
+    if we is not None:
+        w = w * we
     d = Y - T
     return float((w * d * d).sum() / M), 2.0 * w * d / M
 

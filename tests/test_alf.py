@@ -119,3 +119,20 @@ def test_permutation_tables_relabel_consistently(sm):
     old_p = blk.min() // 64
     rel = (blk - 64 * old_p).reshape(8, 8)
     assert (rel == np.arange(64).reshape(8, 8)).all() or (rel == np.arange(64).reshape(8, 8).T).all()
+
+
+def test_committed_network_step_beats_plain_update():
+    """The committed flattening network, evaluated by the FP64 oracle: one
+    step lands closer to the flat parameters than the plain update."""
+    import os
+    from oracle import mlp_oracle as mo
+    gold = os.path.join(os.path.dirname(__file__), "golden")
+    w = np.load(os.path.join(gold, "flat_mlp.npz"))
+    d = np.load(os.path.join(gold, "flat_val.npz"))
+    L = len(w["sizes"]) - 1
+    Ws = [mo.from_bf16_bits(w[f"W{l}_bf16"]) for l in range(L)]
+    bs = [w[f"b{l}"].astype(np.float64) for l in range(L)]
+    X = d["X"].astype(np.float64)
+    _, outs = mo.mlp_forward(X, Ws, bs)
+    dist = alf.distance_to_flat(X, d["Y"], d["W"], outs[-1][1], int(d["samples"]))
+    assert dist["network"] < 0.85 * dist["plain_update"], dist
