@@ -116,6 +116,7 @@ struct PairConst {        // uniform parameters of the pair kernel
   float twoBetaSqrtPi;    // 2*beta/sqrt(pi)
   // VFSWITCH
   float k6, k12, rci3, rci6, dv6, dv12;
+  float k6rci3, k12rci6;  // k6 rc^-3, k12 rc^-6 (the folded switch outside rSwitch)
   // VSWITCH / VSHIFT / FSWITCH / FSHIFT helpers
   float roff2, ron2, rul3inv, rul12;
   float fA, fB, fC, fD, fdvc, rcinv;

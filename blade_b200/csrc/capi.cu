@@ -104,6 +104,8 @@ PairConst make_const(const bnb_params &p) {
   c.k12 = (float)(rc3 * rc3 / (rc3 * rc3 - rs3 * rs3));
   c.rci3 = (float)(1.0 / rc3);
   c.rci6 = (float)(1.0 / (rc3 * rc3));
+  c.k6rci3 = (float)(rc3 / (rc3 - rs3) / rc3);
+  c.k12rci6 = (float)(rc3 * rc3 / (rc3 * rc3 - rs3 * rs3) / (rc3 * rc3));
   double dv6 = 1.0 / (rc3 * rs3);
   c.dv6 = (float)dv6;
   c.dv12 = (float)(dv6 * dv6);

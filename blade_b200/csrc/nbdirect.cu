@@ -209,14 +209,14 @@ __device__ __forceinline__ float plain_pair(const PairConst &pc, float r2, float
   if (ELEC == 1 && VDW == 0) {
     const float t = rcp_approx(fmaf(pc.pBeta, r, 1.0f));
     const float g = ex2_approx(pc.mBeta2Log2e * r2);
-    const float pg = erfcx_poly(t) * g;
-    const float eel = qq * pg * rinv;
+    const float p = erfcx_poly(t);
+    const float qg = qq * g;
     const float rinv2 = rinv * rinv;
     const float rinv3 = rinv2 * rinv;
     const float rinv6 = rinv3 * rinv3;
     const bool in = r < pc.rswitch;
-    const float a = in ? rinv3 : pc.k6 * (rinv3 - pc.rci3);
-    const float b = in ? rinv6 : pc.k12 * (rinv6 - pc.rci6);
+    const float a = in ? rinv3 : fmaf(pc.k6, rinv3, -pc.k6rci3);
+    const float b = in ? rinv6 : fmaf(pc.k12, rinv6, -pc.k12rci6);
     float flr, c12 = 0.f, c6 = 0.f;
     if (COMBINE) {
       const float e6 = ljI.x * ljJ.x;
@@ -238,9 +238,10 @@ __device__ __forceinline__ float plain_pair(const PairConst &pc, float r2, float
     if (ENERGY) {
       const float pe = in ? fmaf(rinv6, rinv6, -pc.dv12) : b * (rinv6 - pc.rci6);
       const float qe = in ? rinv6 - pc.dv6 : a * (rinv3 - pc.rci3);
-      E = eel + (c12 * pe - c6 * qe);
+      E = qg * p * rinv + (c12 * pe - c6 * qe);
     }
-    return (flr - fmaf(qq * pc.twoBetaSqrtPi, g, eel)) * rinv2;
+    // Coulomb part of (dE/dr) r: -qq g (p / r + 2 beta / sqrt(pi))
+    return (flr - qg * fmaf(p, rinv, pc.twoBetaSqrtPi)) * rinv2;
   } else {
     float c12, c6;
     lj_params<COMBINE>(sLJ, rowI, tj, ljI, ljJ, c12, c6);
@@ -297,16 +298,18 @@ __device__ __forceinline__ void plain_loop(JRegs<COMBINE, ALCH> &J, const float4
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     bool act = r2 < pc.rc2;
     if (MASKED) act = act && ((row >> (COMBINE ? J.meta : (J.meta >> 16))) & 1u);
-    if (act) {
-      float E = 0.f;
-      const float fs = plain_pair<ELEC, VDW, ENERGY, COMBINE>(pc, r2, xi.w * J.q, sLJ, rowI, J.meta & 0xFFFF,
-                                                              ljI, make_float2(J.ex, J.er), E);
-      fix = fmaf(fs, dx, fix); fiy = fmaf(fs, dy, fiy); fiz = fmaf(fs, dz, fiz);
-      J.fx = fmaf(-fs, dx, J.fx); J.fy = fmaf(-fs, dy, J.fy); J.fz = fmaf(-fs, dz, J.fz);
-      if (ENERGY) {
-        ei += E;
-        if (count) pairs++;
-      }
+    // Branch-free: the warp evaluates the pair math whenever any of its lanes
+    // is in range, so every lane computes it and lanes out of range (or
+    // excluded) select zero -- no divergent branch to enter and leave.
+    float E = 0.f;
+    float fs = plain_pair<ELEC, VDW, ENERGY, COMBINE>(pc, r2, xi.w * J.q, sLJ, rowI, J.meta & 0xFFFF, ljI,
+                                                      make_float2(J.ex, J.er), E);
+    fs = act ? fs : 0.f;
+    fix = fmaf(fs, dx, fix); fiy = fmaf(fs, dy, fiy); fiz = fmaf(fs, dz, fiz);
+    J.fx = fmaf(-fs, dx, J.fx); J.fy = fmaf(-fs, dy, J.fy); J.fz = fmaf(-fs, dz, J.fz);
+    if (ENERGY) {
+      ei += act ? E : 0.f;
+      if (count) pairs += act ? 1 : 0;
     }
     J.move(rot, gj, MASKED || !COMBINE);
     J.move_forces(rot, gj, false);

@@ -62,3 +62,23 @@ def test_batch_bias_matches_oracle(cuda):
     lo, _ = oracle.bias(lam, fixed, var)
     np.testing.assert_allclose(lf.cpu().numpy(), lo, rtol=1e-6, atol=1e-6)
     B.close()
+
+
+def test_gpu_histograms_equal_trajectory_histograms(cuda):
+    """Histograms accumulated on the GPU during stepping equal those built
+    from the lambda trajectory of the same steps (what ALF reads from .lmd)."""
+    from blade_b200 import lmd
+    reps = [alf.flattening_system(100 + k) for k in range(2)]
+    B = MsldBatch(reps, gamma_ps=5.0, theta_mass=5.0, gamma_theta_ps=1.0)
+    sm = alf.site_map(reps, B.nb.lam_starts)
+    B.enable_histograms(sm.pairs)
+    traj = []
+    for k in range(40):
+        B.enqueue_step(k)
+        traj.append(B.lam.cpu().numpy().copy())
+    h1, h2, he = B.take_histograms()
+    r1, r2, re = lmd.histograms(np.array(traj), sm.pairs, B.fixed.cpu().numpy().astype(bool))
+    np.testing.assert_array_equal(h1, r1)
+    np.testing.assert_array_equal(h2, r2)
+    np.testing.assert_array_equal(he, re)
+    B.close()
