@@ -16,7 +16,7 @@
 //    item, j forces once per tile, energy and dU/dlambda per work item.  The
 //    FP32 partial sums inside a work item have a fixed order, so results do
 //    not depend on which warp, CTA or launch runs which work item.
-//  * Pair math in FP32: rsqrt, erfc as exp(-x^2)*P8(1/(1+p x)) sharing the
+//  * Pair math in FP32: rsqrt, erfc as exp(-x^2)*P6(1/(1+p x)) sharing the
 //    Gaussian with the force (erfc_fit.h), branch-free force switching.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -68,16 +68,14 @@ __device__ __forceinline__ bool aabb_hit(float4 imin, float4 imax, float4 jmin, 
   return acc <= c2;
 }
 
-// erfc(x) exp(x^2) as P8(t), t = 1/(1+p x): even/odd split halves the
+// erfc(x) exp(x^2) as P6(t), t = 1/(1+p x): even/odd split halves the
 // dependency chain of a plain Horner evaluation.
 __device__ __forceinline__ float erfcx_poly(float t) {
   const float t2 = t * t;
-  float pe = fmaf(kErfcC8, t2, kErfcC6);
-  pe = fmaf(pe, t2, kErfcC4);
+  float pe = fmaf(kErfcC6, t2, kErfcC4);
   pe = fmaf(pe, t2, kErfcC2);
   pe = fmaf(pe, t2, kErfcC0);
-  float po = fmaf(kErfcC7, t2, kErfcC5);
-  po = fmaf(po, t2, kErfcC3);
+  float po = fmaf(kErfcC5, t2, kErfcC3);
   po = fmaf(po, t2, kErfcC1);
   return fmaf(po, t, pe);
 }
