@@ -259,7 +259,8 @@ struct JRegs {
   float l;                 // lambda of b
   float fx, fy, fz, fl;
 
-  __device__ __forceinline__ void move(int src, int width, bool withMeta = true) {
+  // withAlch: also the MSLD fields (tiles without MSLD atoms never read them)
+  __device__ __forceinline__ void move(int src, int width, bool withMeta = true, bool withAlch = true) {
     x = __shfl_sync(kFull, x, src, width);
     y = __shfl_sync(kFull, y, src, width);
     z = __shfl_sync(kFull, z, src, width);
@@ -269,7 +270,7 @@ struct JRegs {
       ex = __shfl_sync(kFull, ex, src, width);
       er = __shfl_sync(kFull, er, src, width);
     }
-    if (ALCH) {
+    if (ALCH && withAlch) {
       b = __shfl_sync(kFull, b, src, width);
       l = __shfl_sync(kFull, l, src, width);
     }
@@ -296,20 +297,26 @@ __device__ __forceinline__ void plain_loop(JRegs<COMBINE, ALCH> &J, const float4
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     bool act = r2 < pc.rc2;
     if (MASKED) act = act && ((row >> (COMBINE ? J.meta : (J.meta >> 16))) & 1u);
-    // Branch-free: the warp evaluates the pair math whenever any of its lanes
-    // is in range, so every lane computes it and lanes out of range (or
-    // excluded) select zero -- no divergent branch to enter and leave.
-    float E = 0.f;
-    float fs = plain_pair<ELEC, VDW, ENERGY, COMBINE>(pc, r2, xi.w * J.q, sLJ, rowI, J.meta & 0xFFFF, ljI,
-                                                      make_float2(J.ex, J.er), E);
-    fs = act ? fs : 0.f;
-    fix = fmaf(fs, dx, fix); fiy = fmaf(fs, dy, fiy); fiz = fmaf(fs, dz, fiz);
-    J.fx = fmaf(-fs, dx, J.fx); J.fy = fmaf(-fs, dy, J.fy); J.fz = fmaf(-fs, dz, J.fz);
-    if (ENERGY) {
-      ei += act ? E : 0.f;
-      if (count) pairs += act ? 1 : 0;
+    if (!ENERGY) {
+      // Branch-free: the warp evaluates the pair math whenever any of its
+      // lanes is in range, so every lane computes it and lanes out of range
+      // (or excluded) select zero -- no divergent branch to enter and leave.
+      float E = 0.f;
+      float fs = plain_pair<ELEC, VDW, ENERGY, COMBINE>(pc, r2, xi.w * J.q, sLJ, rowI, J.meta & 0xFFFF, ljI,
+                                                        make_float2(J.ex, J.er), E);
+      fs = act ? fs : 0.f;
+      fix = fmaf(fs, dx, fix); fiy = fmaf(fs, dy, fiy); fiz = fmaf(fs, dz, fiz);
+      J.fx = fmaf(-fs, dx, J.fx); J.fy = fmaf(-fs, dy, J.fy); J.fz = fmaf(-fs, dz, J.fz);
+    } else if (act) {  // energy steps (1 in 10) keep the branch: fewer live registers
+      float E = 0.f;
+      const float fs = plain_pair<ELEC, VDW, ENERGY, COMBINE>(pc, r2, xi.w * J.q, sLJ, rowI, J.meta & 0xFFFF,
+                                                              ljI, make_float2(J.ex, J.er), E);
+      fix = fmaf(fs, dx, fix); fiy = fmaf(fs, dy, fiy); fiz = fmaf(fs, dz, fiz);
+      J.fx = fmaf(-fs, dx, J.fx); J.fy = fmaf(-fs, dy, J.fy); J.fz = fmaf(-fs, dz, J.fz);
+      ei += E;
+      if (count) pairs++;
     }
-    J.move(rot, gj, MASKED || !COMBINE);
+    J.move(rot, gj, MASKED || !COMBINE, false);
     J.move_forces(rot, gj, false);
   }
 }
@@ -446,7 +453,7 @@ __global__ void __launch_bounds__(256, ALCH ? 3 : 4) k_pair(KArgs A) {
       const int cl = lane & (gj - 1);
       const int src = cl < nj ? sIdx[warp][cl] : lane;
       __syncwarp();
-      J.move(src, 32);
+      J.move(src, 32, true, alchTile);
       if (cl >= nj) J.x = 1.0e18f;  // empty compacted slot: never within rCut
       J.fx = J.fy = J.fz = J.fl = 0.f;
       const int rot = lane + 1;
