@@ -577,18 +577,19 @@ __global__ void __launch_bounds__(256, ALCH ? 3 : 4) k_pair(KArgs A) {
 }
 
 // Converts the fixed-point accumulators to the caller's outputs and clears them.
+// One thread per atom, in atom order: the outputs (in the caller's atom
+// order) are written coalesced, and the per-slot accumulators, still in L2
+// from the pair kernel's atomics, are gathered through atomSlot.
 __global__ void k_finalize(Dev d, bnb_outputs o) {
   const int S = 32 * d.maxBlocks;
-  const int B = d.ctr->blockCount;
   const double inv = 1.0 / kFixScale;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 32 * B; t += gridDim.x * blockDim.x) {
-    int a = d.slotAtom[t];
-    if (a < 0) continue;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < d.N; a += gridDim.x * blockDim.x) {
+    const int t = d.atomSlot[a];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-      long long v = d.accF[k * S + t];
-      d.accF[k * S + t] = 0;
-      double f = (double)v * inv;
+      const long long v = d.accF[k * S + t];
+      if (v) d.accF[k * S + t] = 0;
+      const double f = (double)v * inv;
       if (o.force64) o.force64[3 * a + k] = f;
       if (o.force && v) atomicAdd(&o.force[3 * a + k], (float)f);
     }
@@ -800,7 +801,7 @@ int launch_pair(const Dev &d, const PairConst &pc, const float *lambda, int elec
 }
 
 void launch_finalize(const Dev &d, const bnb_outputs &o, cudaStream_t s) {
-  int n = 32 * d.maxBlocks;
+  int n = d.N;
   int grid = (n + 255) / 256;
   if (grid > 148 * 8) grid = 148 * 8;
   if (grid < 1) grid = 1;
