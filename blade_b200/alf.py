@@ -27,7 +27,7 @@ Bias terms of a site with n substituents (global block indices i, j):
 Parameter vector of a site: [b (n), c (P), x (2P), s (2P)], P = n(n-1)/2,
 pairs (i,j) i<j in lexicographic order, ordered terms as (i,j) then (j,i).
 
-Flatness (the criterion both methods are judged by): per site the end-state
+Flatness (the criterion both methods are measured by): per site the end-state
 populations p_i = count(lambda_i > 0.99) / sum over the site; its deviation
 is max_i |p_i - 1/n|.  A replica is flat when every site deviates by at most
 FLAT_TOL and spends at least END_FRAC_MIN of its samples at an end state.
@@ -37,7 +37,7 @@ histograms and the current parameters of a replica (3 sites x 4
 substituents) to the remaining correction, trained on pairs from plain runs
 (target: the plain run's converged parameters minus the current ones).  The
 plain update stays as fallback (non-finite prediction, or flatness worse by
-more than JUDGE_MARGIN after a learned step).
+more than FALLBACK_MARGIN after a learned step).
 """
 from __future__ import annotations
 
@@ -52,7 +52,7 @@ X_L0, S_L0 = -5.56, 0.017
 FLAT_TOL = 0.2
 END_FRAC_MIN = 0.1
 B_STEP = 0.5                        # fraction of the end-state free-energy gap closed per iteration
-JUDGE_MARGIN = 0.15
+FALLBACK_MARGIN = 0.15
 CAP_B, CAP_PAIR = 3.0, 1.0          # kcal/mol per plain iteration
 RIDGE_B, RIDGE_PAIR = 0.01, 0.2
 END_FRAC_TARGET = 0.2               # least fraction of samples at an end state that c keeps
@@ -63,9 +63,9 @@ THETA_MASS = 5.0                    # test/T4L/prep/T4L149F.inp:69,81 (msld init
 
 
 def flattening_system(seed: int):
-    """A config-3 style replica for flattening: the 216-water box with 3 sites x
-    4 substituents of 8-15 atoms (charges ~N(0, 0.35) e, per-atom LJ from the
-    config-3 ranges), sites kept apart.  The 4 substituents of a site are
+    """An MSLD water-box replica for flattening: the 216-water box with 3 sites x
+    4 substituents of 8-15 atoms (charges ~N(0, 0.35) e, per-atom LJ with eps
+    ~U(0.02, 0.2) kcal/mol and Rmin/2 ~U(1.2, 2.1) A), sites kept apart.  The 4 substituents of a site are
     variants of one fragment, as R-groups that differ at a few atoms: one
     shape, charges perturbed by N(0, VARIANT_SIGMA) e, one atom's LJ changed;
     they are rigid (no pairs inside a substituent) and tied atom by atom with
@@ -380,7 +380,8 @@ def run_plain(drv: AlfBatch, n_iter: int, log=None):
 
 
 def run_learned(drv: AlfBatch, model, n_iter: int, log=None):
-    """Learned flattening with the plain update as fallback and judge."""
+    """Learned flattening with the plain update as fallback (non-finite output,
+    or flatness worse by more than FALLBACK_MARGIN after a learned step)."""
     import torch
     check_layout(drv.sm)
     R = drv.sm.n_replicas
@@ -394,7 +395,7 @@ def run_learned(drv: AlfBatch, model, n_iter: int, log=None):
         pred = model.forward(X).cpu().numpy()[:, :N_PARAMS_REP].astype(np.float64) * TARGET_SCALE
         plain = plain_update(drv.sm, h1, h2, he, drv.T)
         learned = pred.reshape(-1)
-        bad = ~np.isfinite(pred).all(1) | (used_learned & (dev > prev_dev + JUDGE_MARGIN))
+        bad = ~np.isfinite(pred).all(1) | (used_learned & (dev > prev_dev + FALLBACK_MARGIN))
         use_plain = np.repeat(bad, N_PARAMS_REP)
         delta = np.where(use_plain, plain, learned)
         recs.append({"params": drv.params.copy(), "dev": dev, "frac": frac, "fallback": bad.copy()})
@@ -443,7 +444,7 @@ def flat_targets(Xseq: np.ndarray):
     consecutive plain iterations of R replicas, each site's target is the
     change from its current parameters to those it had at the first iteration
     its histograms were flat (zero from then on); sites that never became
-    flat get weight 0.  Flatness is judged on the top histogram bin
+    flat get weight 0.  Flatness is measured on the top histogram bin
     (lambda > 31/32) standing in for the end-state count.  Returns
     (Y, W) [T, R, OUT_PAD] with Y scaled by 1/TARGET_SCALE."""
     T, R, _ = Xseq.shape
@@ -549,7 +550,7 @@ def run_sites(drv: AlfBatch, n_iter: int, model=None, scale: float = 1.0, with_p
         else:
             X = torch.from_numpy(replica_features(drv.sm, h1, h2, drv.params)).to(drv.B.dev)
             pred = model.forward(X).cpu().numpy()[:, :N_PARAMS_REP].astype(np.float64) * TARGET_SCALE
-            bad = ~np.isfinite(pred).all(1) | (used_learned & (rdev > prev + JUDGE_MARGIN))
+            bad = ~np.isfinite(pred).all(1) | (used_learned & (rdev > prev + FALLBACK_MARGIN))
             step = scale * pred.reshape(-1) + (plain if with_plain else 0.0)
             delta = np.where(np.repeat(bad, N_PARAMS_REP), plain, step)
             used_learned = ~bad

@@ -321,7 +321,7 @@ def _lj_types(rng, n: int):
 def chain_in_water(seed: int = 2, box: float = 62.23, n_chain: int = 2489, n_wat: int = 7023,
                    rCut: float = 12.0, rSwitch: float = 10.0, beta: float = 0.32,
                    name: str = "chain_water_23558") -> System:
-    """Config-2 system: self-avoiding chain solute + TIP3P water, ~23.5k atoms.
+    """Protein-sized system: self-avoiding chain solute + TIP3P water, ~23.5k atoms.
 
     Chain atoms carry per-atom LJ parameters drawn from U(0.02,0.2) kcal/mol
     and U(1.2,2.1) A, i.e. one LJ type per chain atom.
@@ -435,7 +435,7 @@ def msld_water(seed: int = 3, sites: int = 3, subs: int = 4, clear: float = 2.2,
                avoid_sites: bool = False, charge_sigma: float = 0.35, rigid_substituents: bool = False,
                shared_geometry: bool = False, variant_sigma: float | None = None, variant_lj_atoms: int = 3,
                tie_variants: bool = False) -> System:
-    """Config-3 system: the water box plus MSLD sites anchored on water O's.
+    """MSLD water box: the 216-water box plus MSLD sites anchored on water O's.
 
     Waters with any atom within ``clear`` A of a substituent are removed.
     ``avoid_sites`` keeps substituents of different sites 2.2 A apart (for
@@ -540,7 +540,7 @@ def msld_water(seed: int = 3, sites: int = 3, subs: int = 4, clear: float = 2.2,
 
 def msld_chain(seed: int, n_atoms: int, n_sites: int, subs_per_site, rCut=12.0, rSwitch=10.0,
                beta=0.32) -> System:
-    """Config-4 replica: chain solute + water + MSLD sites on chain atoms, density 0.0965 A^-3."""
+    """MSLD replica: chain solute + water + MSLD sites on chain atoms, density 0.0965 A^-3."""
     rng = np.random.default_rng(seed)
     box = (n_atoms / 0.0965) ** (1 / 3)
     n_chain = max(60, int(0.1 * n_atoms))
@@ -589,7 +589,7 @@ def msld_chain(seed: int, n_atoms: int, n_sites: int, subs_per_site, rCut=12.0, 
 
 
 def batch_replicas(n_rep: int = 64, seed: int = 4, n_min: int = 3000, n_max: int = 30000):
-    """Config-4 batch: sizes log-uniform in [3k, 30k], 1-3 sites x 2-5 substituents."""
+    """Uneven MSLD replicas: sizes log-uniform in [3k, 30k], 1-3 sites x 2-5 substituents."""
     rng = np.random.default_rng(seed)
     out = []
     for r in range(n_rep):
