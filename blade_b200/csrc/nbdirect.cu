@@ -695,7 +695,8 @@ __global__ void __launch_bounds__(128) k_allpairs(AllPairsArgs a) {
     qj = n.q * a.sqrtK;
     tj = n.typeIdx;
   }
-  float fix = 0.f, fiy = 0.f, fiz = 0.f, fjx = 0.f, fjy = 0.f, fjz = 0.f, e = 0.f;
+  float fix = 0.f, fiy = 0.f, fiz = 0.f, fjx = 0.f, fjy = 0.f, fjz = 0.f;
+  long long ef = 0;  // energy in fixed point per pair
   const int src = (lane + 1) & 31;
   for (int k = 0; k < 32; ++k) {
     const int jl = (lane + k) & 31;
@@ -715,7 +716,7 @@ __global__ void __launch_bounds__(128) k_allpairs(AllPairsArgs a) {
         const float sc = dEdr * rinv;
         fix = fmaf(sc, dx, fix); fiy = fmaf(sc, dy, fiy); fiz = fmaf(sc, dz, fiz);
         fjx = fmaf(-sc, dx, fjx); fjy = fmaf(-sc, dy, fjy); fjz = fmaf(-sc, dz, fjz);
-        if (ENERGY) e += E;
+        if (ENERGY) ef += to_fix(E);
       }
     }
     xj = __shfl_sync(0xFFFFFFFFu, xj, src);
@@ -739,7 +740,6 @@ __global__ void __launch_bounds__(128) k_allpairs(AllPairsArgs a) {
     red_add(&a.accF[2 * S + j0], to_fix(fjz));
   }
   if (ENERGY) {
-    long long ef = to_fix(e);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) ef += __shfl_xor_sync(0xFFFFFFFFu, ef, o);
     if (lane == 0 && ef != 0) red_add(a.accE, ef);
