@@ -71,6 +71,9 @@ def lib():
             "bnb_set_tuning": (i, [p, i, i]),
             "bnb_get_tuning": (i, [p, p, p]),
             "bnb_autotune": (i, [p, p, p, p, i, p, p]),
+            "bnb_set_pairs": (i, [p, i, p, i, p, i]),
+            "bnb_compute_nb14": (i, [p, p, p, p, i, p, p]),
+            "bnb_compute_nbex": (i, [p, p, p, p, i, p, p]),
             "bnb_nbdirect_noalloc": (i, [p, i, p, p, p, i, p, p, p, i, p, p]),
             "bnb_mlp_linear_forward": (i, [i, i, i, p, p, p, i, p, p, p, p]),
             "bnb_mlp_linear_backward": (i, [i, i, i, p, p, i, p, p, p, p, p, p, p, p]),

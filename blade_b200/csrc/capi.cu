@@ -21,6 +21,7 @@
 #include "erfc_fit.h"
 #include "listbuild.h"
 #include "nbdirect.h"
+#include "pairs.h"
 
 using bnb::Dev;
 using bnb::PairConst;
@@ -60,6 +61,13 @@ struct bnb_handle {
   size_t listBytes = 0;
   int *colRep_d = nullptr;
   PairConst pc{};
+  // nb14 / nbex lists (bnb_set_pairs)
+  void *pairArena = nullptr;
+  int n14 = 0, nex = 0;
+  bool soft14 = false;
+  bnb_nb14 *nb14_d = nullptr;
+  bnb_nbex *nbex_d = nullptr;
+  long long *accP = nullptr, *accPL = nullptr, *accPE = nullptr;
 };
 
 namespace {
@@ -341,6 +349,7 @@ int bnb_destroy(bnb_handle *h) {
   if (!h) return BNB_ERR_ARG;
   free_list(h);
   if (h->topoArena) cudaFree(h->topoArena);
+  if (h->pairArena) cudaFree(h->pairArena);
   destroy_events(h);
   delete h;
   return BNB_OK;
@@ -937,3 +946,113 @@ extern "C" int bnb_nbdirect_noalloc(const bnb_params *p, int atomCount, const fl
   a.accE = scratch + 3 * BNB_NOALLOC_MAX_ATOMS;
   return bnb::launch_allpairs(a, *out, p->elecMethod, p->vdwMethod, calcEnergy != 0, s);
 }
+
+// ---------------------------------------------------------------------------
+// nb14 / nbex pair lists (getforce_nb14 / getforce_nbex, src/bonded/pair.cu)
+// ---------------------------------------------------------------------------
+namespace {
+int pairs_boxes(bnb_handle *h, const float *boxes, cudaStream_t s) {
+  bool changed = false;
+  for (int r = 0; r < h->R; r++)
+    for (int k = 0; k < 3; k++)
+      if (h->rep[r].box[k] != boxes[3 * r + k]) {
+        h->rep[r].box[k] = boxes[3 * r + k];
+        changed = true;
+      }
+  return changed ? upload_rep(h, s) : BNB_OK;
+}
+
+bnb::PairsArgs pairs_args(bnb_handle *h, const float *position, const float *lambda) {
+  bnb::PairsArgs a{};
+  a.N = h->N;
+  a.R = h->R;
+  a.lamTotal = h->lamTotal;
+  a.n14 = h->n14;
+  a.nex = h->nex;
+  a.rCut = h->p.rCut;
+  a.rSwitch = h->p.rSwitch;
+  a.beta = h->p.betaEwald;
+  a.kElectric = h->p.kElectric;
+  a.softR = h->p.softCoreRadius;
+  a.x = position;
+  a.lambda = lambda;
+  a.atomRep = h->d.atomRep;
+  a.rep = h->d.rep;
+  a.nb14 = h->nb14_d;
+  a.nbex = h->nbex_d;
+  a.accF = h->accP;
+  a.accL = h->accPL;
+  a.accE = h->accPE;
+  return a;
+}
+}  // namespace
+
+extern "C" int bnb_set_pairs(bnb_handle *h, int nb14Count, const bnb_nb14 *nb14, int nbexCount,
+                             const bnb_nbex *nbex, int useSoftCore14) {
+  if (!h || nb14Count < 0 || nbexCount < 0 || (nb14Count && !nb14) || (nbexCount && !nbex)) return BNB_ERR_ARG;
+  if (!h->topo) return BNB_ERR_STATE;
+  std::vector<int> atomRep(h->N);
+  for (int r = 0; r < h->R; r++)
+    for (int i = h->atomStart[r]; i < h->atomStart[r + 1]; i++) atomRep[i] = r;
+  auto okPair = [&](const int idx[2], const int sb[2]) {
+    if (idx[0] < 0 || idx[0] >= h->N || idx[1] < 0 || idx[1] >= h->N) return false;
+    if (atomRep[idx[0]] != atomRep[idx[1]]) return false;
+    for (int k = 0; k < 2; k++)
+      if ((sb[k] & 0xFFFF) >= h->lamTotal) return false;
+    return true;
+  };
+  for (int t = 0; t < nb14Count; t++)
+    if (!okPair(nb14[t].idx, nb14[t].siteBlock)) return BNB_ERR_ARG;
+  for (int t = 0; t < nbexCount; t++)
+    if (!okPair(nbex[t].idx, nbex[t].siteBlock)) return BNB_ERR_ARG;
+  if (h->pairArena) cudaFree(h->pairArena);
+  h->pairArena = nullptr;
+  Arena a;
+  size_t o14 = a.take<bnb_nb14>(std::max(nb14Count, 1)), oex = a.take<bnb_nbex>(std::max(nbexCount, 1)),
+         of = a.take<long long>(3 * (size_t)std::max(h->N, 1)), ol = a.take<long long>(std::max(h->lamTotal, 1)),
+         oe = a.take<long long>(std::max(h->R, 1));
+  void *base = nullptr;
+  if (!ok(cudaMalloc(&base, a.off))) return BNB_ERR_CUDA;
+  h->pairArena = base;
+  char *b = static_cast<char *>(base);
+  h->nb14_d = (bnb_nb14 *)(b + o14);
+  h->nbex_d = (bnb_nbex *)(b + oex);
+  h->accP = (long long *)(b + of);
+  h->accPL = (long long *)(b + ol);
+  h->accPE = (long long *)(b + oe);
+  if (!ok(cudaMemset(base, 0, a.off))) return BNB_ERR_CUDA;
+  if (nb14Count && !ok(cudaMemcpy(h->nb14_d, nb14, sizeof(bnb_nb14) * nb14Count, cudaMemcpyHostToDevice)))
+    return BNB_ERR_CUDA;
+  if (nbexCount && !ok(cudaMemcpy(h->nbex_d, nbex, sizeof(bnb_nbex) * nbexCount, cudaMemcpyHostToDevice)))
+    return BNB_ERR_CUDA;
+  h->n14 = nb14Count;
+  h->nex = nbexCount;
+  h->soft14 = useSoftCore14 != 0;
+  return BNB_OK;
+}
+
+extern "C" int bnb_compute_nb14(bnb_handle *h, const float *position, const float *lambda, const float *boxes,
+                                int calcEnergy, const bnb_outputs *out, void *stream) {
+  if (!h || !out || !boxes || (h->N > 0 && !position)) return BNB_ERR_ARG;
+  if (!h->pairArena) return BNB_ERR_STATE;
+  if (h->alch && !lambda) return BNB_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = pairs_boxes(h, boxes, s);
+  if (rc) return rc;
+  bnb::PairsArgs a = pairs_args(h, position, lambda);
+  return bnb::launch_nb14(a, *out, h->p.elecMethod, h->p.vdwMethod, h->soft14 && h->alch, calcEnergy != 0, s);
+}
+
+extern "C" int bnb_compute_nbex(bnb_handle *h, const float *position, const float *lambda, const float *boxes,
+                                int calcEnergy, const bnb_outputs *out, void *stream) {
+  if (!h || !out || !boxes || (h->N > 0 && !position)) return BNB_ERR_ARG;
+  if (!h->pairArena) return BNB_ERR_STATE;
+  if (h->alch && !lambda) return BNB_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = pairs_boxes(h, boxes, s);
+  if (rc) return rc;
+  bnb::PairsArgs a = pairs_args(h, position, lambda);
+  if (h->p.elecMethod != 1) a.nex = 0;  // the correction exists for PME only (pair.cu:379)
+  return bnb::launch_nbex(a, *out, calcEnergy != 0, s);
+}
+

@@ -117,6 +117,46 @@ class NbDirect:
         _lib.call("bnb_compute", self.h, _ptr(positions), _ptr(lambdas), b.ctypes.data_as(C.c_void_p),
                   int(bool(calc_energy)), C.byref(out), _stream(stream))
 
+    # -- nb14 / nbex pair lists (getforce_nb14 / getforce_nbex) ---------------------
+    def set_pairs(self, soft14: bool = False):
+        """Uploads every replica's ``nb14`` / ``nbex`` lists (bnb_set_pairs),
+        with atom and block indices shifted to the concatenated layout."""
+        from .systems import NB14_DTYPE, NBEX_DTYPE
+        n14, nex = [], []
+        for r, s in enumerate(self.systems):
+            for src, dst, dt in ((s.nb14, n14, NB14_DTYPE), (s.nbex, nex, NBEX_DTYPE)):
+                if src is None or len(src) == 0:
+                    continue
+                a = np.array(src, dt)
+                a["idx"] += int(self.starts[r])
+                blk = a["siteBlock"] & 0xFFFF
+                a["siteBlock"] = np.where(blk != 0, (a["siteBlock"] & ~0xFFFF) | (blk + int(self.lam_starts[r])), 0)
+                dst.append(a)
+        a14 = np.ascontiguousarray(np.concatenate(n14) if n14 else np.zeros(0, NB14_DTYPE))
+        aex = np.ascontiguousarray(np.concatenate(nex) if nex else np.zeros(0, NBEX_DTYPE))
+        _lib.call("bnb_set_pairs", self.h, len(a14), a14.ctypes.data_as(C.c_void_p) if len(a14) else None,
+                  len(aex), aex.ctypes.data_as(C.c_void_p) if len(aex) else None, int(bool(soft14)))
+
+    def getforce_pairs(self, which: str, positions, lambdas=None, calc_energy=True, force=None,
+                       lambda_force=None, energy=None, force64=None, lambda_force64=None, energy64=None,
+                       stream=None, boxes=None):
+        """bnb_compute_nb14 (which="nb14") or bnb_compute_nbex (which="nbex")."""
+        out = _lib.Outputs(force=_ptr(force), lambdaForce=_ptr(lambda_force), energy=_ptr(energy),
+                           force64=_ptr(force64), lambdaForce64=_ptr(lambda_force64), energy64=_ptr(energy64))
+        b = np.ascontiguousarray(self.boxes if boxes is None else boxes, np.float32)
+        _lib.call("bnb_compute_" + which, self.h, _ptr(positions), _ptr(lambdas), b.ctypes.data_as(C.c_void_p),
+                  int(bool(calc_energy)), C.byref(out), _stream(stream))
+
+    def evaluate_pairs(self, which: str, positions=None, lambdas=None, calc_energy=True):
+        import torch
+        pos = self.positions_tensor() if positions is None else positions
+        lam = self.lambdas_tensor() if lambdas is None else lambdas
+        f64 = torch.zeros(3 * self.N, dtype=torch.float64, device=self.device)
+        l64 = torch.zeros(self.L, dtype=torch.float64, device=self.device)
+        e64 = torch.zeros(self.R, dtype=torch.float64, device=self.device)
+        self.getforce_pairs(which, pos, lam, calc_energy, force64=f64, lambda_force64=l64, energy64=e64)
+        return f64.reshape(-1, 3), l64, e64
+
     # -- conveniences ------------------------------------------------------------
     def positions_tensor(self, xyz_list=None):
         import torch

@@ -36,6 +36,10 @@ TIP3P_EPS_H, TIP3P_RH_H = 0.046, 0.2245
 TIP3P_ROH, TIP3P_THETA = 0.9572, math.radians(104.52)
 
 NBOND_DTYPE = np.dtype([("siteBlock", "<i4"), ("q", "<f4"), ("typeIdx", "<i4")])
+# Same layouts as struct Nb14Potential / NbExPotential, src/system/potential.h:91-104.
+NB14_DTYPE = np.dtype([("idx", "<i4", 2), ("siteBlock", "<i4", 2), ("qxq", "<f4"), ("c12", "<f4"), ("c6", "<f4"),
+                       ("e14fac", "<f4")])
+NBEX_DTYPE = np.dtype([("idx", "<i4", 2), ("siteBlock", "<i4", 2), ("qxq", "<f4")])
 
 
 @dataclasses.dataclass
@@ -65,6 +69,8 @@ class System:
     vdwMethod: int = 0           # VFSWITCH
     msld: Msld | None = None
     cullPad: float = 2.0
+    nb14: np.ndarray | None = None       # NB14_DTYPE 1-4 pairs (with_pair_lists)
+    nbex: np.ndarray | None = None       # NBEX_DTYPE excluded pairs for the PME correction
     bonds: np.ndarray | None = None      # [B,2] int32 covalent bonds (one order), for dynamics only
     bond_param: np.ndarray | None = None  # [B,2] float32 (kb, b0): U = kb/2 (r - b0)^2
 
@@ -611,3 +617,60 @@ def excl_csr(N: int, excl: np.ndarray):
     start = np.zeros(N + 1, np.int64)
     np.add.at(start, e[:, 0] + 1, 1)
     return np.cumsum(start).astype(np.int32), e[:, 1].astype(np.int32)
+
+
+def _pair_site_blocks(a: int, b: int):
+    """(siteBlock[0], siteBlock[1]) of a pair as the pair kernel reads them
+    (src/bonded/pair.cu:224-231): the perturbed block first, the second slot
+    only for two blocks of different sites; None for two blocks of one site
+    (mutually excluded, never present together)."""
+    if a == b:
+        return (a, 0)
+    if a == 0 or b == 0:
+        return (a or b, 0)
+    if (a >> 16) == (b >> 16):
+        return None
+    return (a, b)
+
+
+def with_pair_lists(s: System, e14fac: float = 1.0) -> System:
+    """Copy of ``s`` with 1-4 pair lists (Potential::nb14s, src/system/potential.cxx:1093-1140)
+    and PME exclusion-correction lists (Potential::nbexs, potential.cxx:1144-1160).
+
+    1-4 pairs are (i, i+3) along runs of consecutive bonded atoms of one block
+    ((i,i+1), (i+1,i+2), (i+2,i+3) all excluded); they join the exclusions of
+    the direct space and get c12/c6 from the LJ table and the given e14fac.
+    The correction list holds every other excluded pair i<j.
+    """
+    import dataclasses as dc
+    ex = set(map(tuple, np.asarray(s.excl).tolist()))
+    sb = s.nbonds["siteBlock"]
+    q = s.nbonds["q"].astype(np.float64)
+    t = s.nbonds["typeIdx"]
+    p14 = []
+    for i in range(s.N - 3):
+        if all((i + k, i + k + 1) in ex for k in range(3)) and len({int(sb[i + k]) for k in range(4)}) == 1:
+            p14.append((i, i + 3))
+    nb14 = np.zeros(len(p14), NB14_DTYPE)
+    for n, (i, j) in enumerate(p14):
+        nb14[n]["idx"] = (i, j)
+        nb14[n]["siteBlock"] = _pair_site_blocks(int(sb[i]), int(sb[j]))
+        nb14[n]["qxq"] = np.float32(q[i] * q[j])
+        nb14[n]["c12"], nb14[n]["c6"] = s.vdw[t[i], t[j]]
+        nb14[n]["e14fac"] = e14fac
+    excl = np.asarray(s.excl)
+    if p14:
+        a = np.array(p14, np.int32)
+        excl = np.unique(np.concatenate([excl, a, a[:, ::-1]]), axis=0)
+    s14 = set(p14)
+    rows = []
+    for i, j in excl.tolist():
+        if i < j and (i, j) not in s14:
+            blocks = _pair_site_blocks(int(sb[i]), int(sb[j]))
+            if blocks is not None:
+                rows.append(((i, j), blocks, np.float32(q[i] * q[j])))
+    nbex = np.zeros(len(rows), NBEX_DTYPE)
+    for n, (ij, blocks, qq) in enumerate(rows):
+        nbex[n]["idx"], nbex[n]["siteBlock"], nbex[n]["qxq"] = ij, blocks, qq
+    return dc.replace(s, name=s.name + "_pairs", excl=excl.astype(np.int32), nb14=nb14, nbex=nbex)
+

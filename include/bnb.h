@@ -43,6 +43,9 @@ extern "C" {
 typedef struct { int siteBlock; float q; int typeIdx; } bnb_nbond;
 /* Same layout as struct VdwPotential, src/system/potential.h:112-114. */
 typedef struct { float c12, c6; } bnb_vdw;
+/* Same layouts as struct Nb14Potential / NbExPotential, src/system/potential.h:91-104. */
+typedef struct { int idx[2]; int siteBlock[2]; float qxq, c12, c6, e14fac; } bnb_nb14;
+typedef struct { int idx[2]; int siteBlock[2]; float qxq; } bnb_nbex;
 /* Same layout as struct VariableBias, src/msld/msld.h:13-19. */
 typedef struct { int i, j, type; float l0, k; int n; } bnb_varbias;
 
@@ -186,6 +189,28 @@ int bnb_nbdirect_noalloc(const bnb_params *p, int atomCount, const float *positi
                          const float *box, const bnb_nbond *nbonds, int typeCount,
                          const bnb_vdw *vdw, const int *exclStart, const int *exclAtom,
                          int calcEnergy, const bnb_outputs *out, void *stream);
+
+/*
+ * 1-4 pairs and the PME correction of excluded pairs (getforce_nb14 and
+ * getforce_nbex, src/bonded/pair.cu:288-398; the lists Potential::nb14s and
+ * Potential::nbexs, src/system/potential.cxx:1093-1160).  bnb_set_pairs
+ * copies the host lists (atom indices of the concatenated replicas, both
+ * atoms in one replica; siteBlock as the reference's nb14_scaling /
+ * nbex_scaling leave them, with the block part (low 16 bits) indexing the
+ * concatenated lambda blocks of all replicas) and allocates their
+ * accumulators (BNB_ERR_ARG for an index out of range); useSoftCore14 is
+ * Msld::useSoftCore14.  bnb_compute_nb14 / bnb_compute_nbex evaluate one list
+ * on position (device float [3N]) and lambda (device float, State::lambda_fd)
+ * into `out` with bnb_compute's output semantics; energies are the eenb14 and
+ * eenbrecipexcl terms.  The nbex call does no pair work unless elecMethod is
+ * PME (as the reference).  The list of a handle need not be built.
+ */
+int bnb_set_pairs(bnb_handle *h, int nb14Count, const bnb_nb14 *nb14, int nbexCount,
+                  const bnb_nbex *nbex, int useSoftCore14);
+int bnb_compute_nb14(bnb_handle *h, const float *position, const float *lambda,
+                     const float *boxes, int calcEnergy, const bnb_outputs *out, void *stream);
+int bnb_compute_nbex(bnb_handle *h, const float *position, const float *lambda,
+                     const float *boxes, int calcEnergy, const bnb_outputs *out, void *stream);
 
 /*
  * Sets list capacities (candidate tiles, 32-row exclusion masks, work items)

@@ -259,3 +259,30 @@ def active_tiles(lst, bmin, bmax, box, rcut):
                                              _ptr(np.ascontiguousarray(bmax[j])),
                                              _ptr(np.ascontiguousarray(s, np.float32)), C.c_float(c2)))
     return out
+
+
+NB14_DTYPE = np.dtype([("idx", "<i4", 2), ("siteBlock", "<i4", 2), ("qxq", "<f4"), ("c12", "<f4"), ("c6", "<f4"),
+                       ("e14fac", "<f4")])
+NBEX_DTYPE = np.dtype([("idx", "<i4", 2), ("siteBlock", "<i4", 2), ("qxq", "<f4")])
+
+
+def pair_lists(sys, xyz=None, lam=None, which="nb14", soft14=False):
+    """FP64 nb14 or nbex energy, gradient dU/dx [N,3] and dU/dlambda
+    (src/bonded/pair.cu) for the system's pair lists."""
+    xyz = np.ascontiguousarray(sys.xyz if xyz is None else xyz, np.float64)
+    box = np.ascontiguousarray(sys.box, np.float64)
+    lam = np.ascontiguousarray(sys.lambdas() if lam is None else lam, np.float64)
+    g = np.zeros((xyz.shape[0], 3))
+    lf = np.zeros(len(lam))
+    e = np.zeros(1)
+    p = params(sys, True)
+    if which == "nb14":
+        pp = np.ascontiguousarray(sys.nb14, NB14_DTYPE)
+        lib().orc_nb14_pairs(len(pp), _ptr(pp), _ptr(xyz), _ptr(box), _ptr(lam), C.byref(p), int(soft14),
+                             _ptr(g), _ptr(lf), _ptr(e))
+    else:
+        pp = np.ascontiguousarray(sys.nbex, NBEX_DTYPE)
+        lib().orc_nbex_pairs(len(pp), _ptr(pp), _ptr(xyz), _ptr(box), _ptr(lam), C.byref(p), _ptr(g), _ptr(lf),
+                             _ptr(e))
+    return {"grad": g, "lambdaForce": lf, "energy": float(e[0])}
+

@@ -449,3 +449,140 @@ void orc_bias(int blockCount, const double *lambda, const double *fixedBias,
   }
   if (energy) *energy += e;
 }
+
+/* ===========================================================================
+ * nb14 / nbex pair lists: FP64 restatement of src/bonded/pair.cu.
+ * ======================================================================== */
+
+/* function_pair(Nb14Potential...), pair.cu:63-187: dE/dr and E. */
+static void nb14_terms(const orc_nb14 *pp, const orc_params *p, double r, double *fpair, double *E) {
+  *fpair = 0;
+  *E = 0;
+  if (!(r < p->rCut)) return;
+  const double rinv = 1 / r, rinv3 = rinv * rinv * rinv, rinv6 = rinv3 * rinv3;
+  const double c12 = pp->c12, c6 = pp->c6, rc = p->rCut, rs = p->rSwitch;
+  if (p->vdwMethod == 0) { /* VFSWITCH, pair.cu:70-93 */
+    const double rc3 = rc * rc * rc, rc6 = rc3 * rc3, rs3 = rs * rs * rs, rs6 = rs3 * rs3;
+    const double k6 = rc3 / (rc3 - rs3), k12 = rc6 / (rc6 - rs6);
+    const int in = r < rs;
+    const double A6 = in ? 1 : k6, A12 = in ? 1 : k12, B6 = in ? 0 : 1 / rc3, B12 = in ? 0 : 1 / rc6;
+    *fpair = 6 * c6 * A6 * (rinv3 - B6) * rinv3 * rinv - 12 * c12 * A12 * (rinv6 - B12) * rinv6 * rinv;
+    const double CC6 = in ? -1 / rc6 : 0, CC12 = in ? -1 / (rc6 * rc6) : 0;
+    *E = c12 * (A12 * (rinv6 - B12) * (rinv6 - B12) + CC12) - c6 * (A6 * (rinv3 - B6) * (rinv3 - B6) + CC6);
+  } else if (p->vdwMethod == 1) { /* VSWITCH, pair.cu:94-106 (force expression as written) */
+    const double c2of = rc * rc, c2on = rs * rs;
+    const double rul3 = (c2of - c2on) * (c2of - c2on) * (c2of - c2on), rul12 = 12 / rul3;
+    const double rijl = c2on - r * r, riju = c2of - r * r;
+    const double fsw = r < rs ? 1 : riju * riju * (riju - 3 * rijl) / rul3;
+    const double dfsw = r < rs ? 0 : rijl * riju * rul12;
+    *fpair = fsw * (6 * c6 - 12 * c12 * rinv6) * rinv6 * rinv + dfsw * (c12 * rinv6 - c6) * rinv6;
+    *E = fsw * (c12 * rinv6 - c6) * rinv6;
+  } else { /* VSHIFT, pair.cu:107-133 (as written) */
+    const double r2 = r * r, r5 = r2 * r2 * r, r6 = r2 * r2 * r2;
+    const double rinv7 = rinv6 * rinv, rinv12 = rinv6 * rinv6, rinv13 = rinv12 * rinv;
+    const double rc2 = rc * rc, rc6 = rc2 * rc2 * rc2, rc12 = rc6 * rc6, rc18 = rc12 * rc6;
+    *fpair = 6 * c6 * (rinv7 - r5 / rc12) - 12 * c12 * (rinv13 + r5 / rc18);
+    *E = c12 * (rinv12 + 2 * r6 / rc18 - 3 / rc12) - c6 * (rinv6 + r6 / rc12 - 2 / rc6);
+  }
+  const double kqq = p->kElectric * pp->qxq;
+  if (p->elecMethod == 0) { /* FSWITCH, pair.cu:136-156 */
+    const double kqqe14 = kqq * pp->e14fac;
+    const double roff2 = rc * rc, ron2 = rs * rs;
+    const double ginv = 1 / ((roff2 - ron2) * (roff2 - ron2) * (roff2 - ron2));
+    const double A = roff2 * roff2 * (roff2 - 3 * ron2) * ginv, B = 6 * roff2 * ron2 * ginv;
+    const double Cc = -(ron2 + roff2) * ginv, D = 2 * ginv / 5;
+    const double dvc = 8 * (ron2 * roff2 * (rc - rs) - (roff2 * roff2 * rc - ron2 * ron2 * rs) / 5) * ginv;
+    const double r2 = r * r, r3 = r2 * r, r5 = r3 * r2;
+    *fpair += r <= rs ? -kqqe14 * rinv * rinv : -kqqe14 * rinv * (A * rinv + B * r + 3 * Cc * r3 + 5 * D * r5);
+    *E += r <= rs ? kqqe14 * (rinv + dvc)
+                  : kqqe14 * (A * (rinv - 1 / rc) + B * (rc - r) + Cc * (roff2 * rc - r3) + D * (roff2 * roff2 * rc - r5));
+  } else if (p->elecMethod == 1) { /* PME, pair.cu:157-165: erfc(br) + e14fac - 1 */
+    const double br = p->betaEwald * r;
+    const double erfcrinv = (erfc(br) + pp->e14fac - 1) * rinv;
+    *fpair += kqq * (-erfcrinv - 2 / sqrt(M_PI) * p->betaEwald * exp(-br * br)) * rinv;
+    *E += kqq * erfcrinv;
+  } else { /* FSHIFT, pair.cu:166-174 */
+    const double kqqe14 = kqq * pp->e14fac, roffinv = 1 / rc;
+    *fpair += -kqqe14 * (rinv * rinv - roffinv * roffinv);
+    *E += kqqe14 * (rinv - 2 * roffinv + r * roffinv * roffinv);
+  }
+}
+
+static void pl_min_image(const double *xi, const double *xj, const double box[3], double d[3]) {
+  for (int k = 0; k < 3; k++) {
+    double v = xi[k] - xj[k];
+    v -= box[k] * nearbyint(v / box[k]);
+    d[k] = v;
+  }
+}
+
+/* getforce_pair_kernel's scaling, soft core and routing (pair.cu:205-283). */
+static void pair_apply(int ii, int jj, const int sb[2], const double d[3], double r, double rEff, double dredr,
+                       double dredll, int soft, double fpair, double E, const double *lambda, double *grad,
+                       double *lambdaForce, double *energy) {
+  int b0 = 0xFFFF & sb[0], b1 = 0xFFFF & sb[1];
+  double l0 = 1, l1 = 1;
+  if (b0) {
+    l0 = lambda[b0];
+    if (b1) l1 = lambda[b1];
+  }
+  (void)rEff;
+  fpair *= l0 * l1;
+  if (b0) {
+    const double fl = soft ? E + fpair * dredll : E;
+    lambdaForce[b0] += l1 * fl;
+    if (b1) lambdaForce[b1] += l0 * fl;
+  }
+  if (soft) fpair *= dredr;
+  for (int k = 0; k < 3; k++) {
+    grad[3 * ii + k] += fpair / r * d[k];
+    grad[3 * jj + k] -= fpair / r * d[k];
+  }
+  energy[0] += E * l0 * l1;
+}
+
+void orc_nb14_pairs(int n, const orc_nb14 *pp, const double *xyz, const double box[3], const double *lambda,
+                    const orc_params *p, int useSoftCore14, double *grad, double *lambdaForce, double *energy) {
+  for (int t = 0; t < n; t++) {
+    const int ii = pp[t].idx[0], jj = pp[t].idx[1];
+    double d[3];
+    pl_min_image(xyz + 3 * ii, xyz + 3 * jj, box, d);
+    const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    int b0 = 0xFFFF & pp[t].siteBlock[0], b1 = 0xFFFF & pp[t].siteBlock[1];
+    double l0 = 1, l1 = 1;
+    if (b0) {
+      l0 = lambda[b0];
+      if (b1) l1 = lambda[b1];
+    }
+    double rEff = r, dredr = 1, dredll = 0;
+    if (useSoftCore14 && b0) { /* pair.cu:240-254 */
+      const double rSoft = p->softCoreRadius * (1 - l0 * l1);
+      if (r < rSoft) {
+        const double q = r / rSoft;
+        rEff = (1 - 0.5 * q) * q * q * q + 0.5;
+        dredr = (3 - 2 * q) * q * q;
+        dredll = -p->softCoreRadius * (rEff - dredr * q);
+        rEff *= rSoft;
+      }
+    }
+    double fpair, E;
+    nb14_terms(&pp[t], p, rEff, &fpair, &E);
+    pair_apply(ii, jj, pp[t].siteBlock, d, r, rEff, dredr, dredll, useSoftCore14, fpair, E, lambda, grad,
+               lambdaForce, energy);
+  }
+}
+
+void orc_nbex_pairs(int n, const orc_nbex *pp, const double *xyz, const double box[3], const double *lambda,
+                    const orc_params *p, double *grad, double *lambdaForce, double *energy) {
+  for (int t = 0; t < n; t++) {
+    const int ii = pp[t].idx[0], jj = pp[t].idx[1];
+    double d[3];
+    pl_min_image(xyz + 3 * ii, xyz + 3 * jj, box, d);
+    const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    /* function_pair(NbExPotential...), pair.cu:190-202: -kqq erf(br)/r */
+    const double br = p->betaEwald * r, kqq = p->kElectric * pp[t].qxq;
+    const double fpair = kqq * (erf(br) / r - 2 / sqrt(M_PI) * p->betaEwald * exp(-br * br)) / r;
+    const double E = -kqq * erf(br) / r;
+    pair_apply(ii, jj, pp[t].siteBlock, d, r, r, 1, 0, 0, fpair, E, lambda, grad, lambdaForce, energy);
+  }
+}

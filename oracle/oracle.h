@@ -146,6 +146,26 @@ void orc_shift_vector(int code, int *sx, int *sy, int *sz);
 int orc_aabb_hit(const float *imin, const float *imax, const float *jmin,
                  const float *jmax, const float shift[3], float c2);
 
+/* ---- nb14 / nbex pair lists (src/bonded/pair.cu:63-286) ---------------- */
+/* Same layouts as struct Nb14Potential / NbExPotential, src/system/potential.h:91-104. */
+typedef struct { int idx[2]; int siteBlock[2]; float qxq, c12, c6, e14fac; } orc_nb14;
+typedef struct { int idx[2]; int siteBlock[2]; float qxq; } orc_nbex;
+
+/*
+ * FP64 restatement of getforce_pair_kernel with function_pair for
+ * Nb14Potential (pair.cu:63-187: switched LJ and e14fac-scaled elec) and for
+ * NbExPotential (pair.cu:190-202: the PME erf correction of excluded pairs),
+ * MSLD scaling l0*l1 and, for nb14 with useSoftCore14, the soft core
+ * (pair.cu:205-283).  Minimum image in the orthorhombic box.  Outputs are
+ * ADDED: grad[3N] (dU/dx), lambdaForce, energy[1].
+ */
+void orc_nb14_pairs(int n, const orc_nb14 *pp, const double *xyz, const double box[3],
+                    const double *lambda, const orc_params *p, int useSoftCore14,
+                    double *grad, double *lambdaForce, double *energy);
+void orc_nbex_pairs(int n, const orc_nbex *pp, const double *xyz, const double box[3],
+                    const double *lambda, const orc_params *p,
+                    double *grad, double *lambdaForce, double *energy);
+
 #ifdef __cplusplus
 }
 #endif

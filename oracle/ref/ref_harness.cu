@@ -12,7 +12,8 @@
 // src/holonomic, State::broadcast_position/broadcast_box from src/system).
 // Each step it calls Domdec::update_domdec and getforce_nbdirect exactly as
 // Run::dynamics and Potential::calc_force do (src/run/run.cu:554-564,
-// src/system/potential.cxx:1839-1929), on one stream.
+// src/system/potential.cxx:1839-1929), on one stream; ref_evaluate_pairs
+// calls getforce_nb14 / getforce_nbex (src/bonded/pair.cu) the same way.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -23,6 +24,7 @@
 #include <map>
 #include <new>
 
+#include "bonded/pair.h"
 #include "domdec/domdec.h"
 #include "main/defines.h"
 #include "msld/msld.h"
@@ -272,3 +274,45 @@ extern "C" int ref_list_info(ref_handle *h, int *blocks, int *maxPartners) {
   if (maxPartners) *maxPartners = d->maxPartnersPerBlock;
   return 0;
 }
+
+// nb14 / nbex lists (host arrays in the layouts of Nb14Potential /
+// NbExPotential) into Potential, and Msld::useSoftCore14.
+extern "C" int ref_set_pairs(ref_handle *h, int n14, const void *nb14, int nex, const void *nbex, int soft14) {
+  Potential *pot = h->pot;
+  pot->nb14Count = n14;
+  pot->nbexCount = nex;
+  cudaMalloc(&pot->nb14s_d, sizeof(Nb14Potential) * (n14 > 0 ? n14 : 1));
+  cudaMalloc(&pot->nbexs_d, sizeof(NbExPotential) * (nex > 0 ? nex : 1));
+  if (n14) cudaMemcpy(pot->nb14s_d, nb14, sizeof(Nb14Potential) * n14, cudaMemcpyHostToDevice);
+  if (nex) cudaMemcpy(pot->nbexs_d, nbex, sizeof(NbExPotential) * nex, cudaMemcpyHostToDevice);
+  h->msld->useSoftCore14 = soft14 != 0;
+  h->run->calcTermFlag[eenb14] = true;
+  h->run->calcTermFlag[eenbrecipexcl] = true;
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// One nb14 (which 0) or nbex (which 1) evaluation on the current state.
+extern "C" int ref_evaluate_pairs(ref_handle *h, int which, int calcEnergy, double *grad, double *energy,
+                                  double *lambdaForce) {
+  System *sys = h->sys;
+  State *st = h->st;
+  st->broadcast_position(sys);
+  cudaMemsetAsync(st->forceBuffer_d, 0, sizeof(float) * (3 * h->N + 2 * h->nL), h->stream);
+  cudaMemsetAsync(st->energy_d, 0, sizeof(double) * eeend, h->stream);
+  if (which == 0) getforce_nb14(sys, calcEnergy != 0);
+  else getforce_nbex(sys, calcEnergy != 0);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return 2;
+  int n = 3 * h->N;
+  float *tmp = (float *)malloc(sizeof(float) * (n + h->nL));
+  cudaMemcpy(tmp, st->force_d, sizeof(float) * n, cudaMemcpyDeviceToHost);
+  for (int i = 0; i < n; i++) grad[i] = tmp[i];
+  if (lambdaForce) {
+    cudaMemcpy(tmp, st->lambdaForce_d, sizeof(float) * h->nL, cudaMemcpyDeviceToHost);
+    for (int i = 0; i < h->nL; i++) lambdaForce[i] = tmp[i];
+  }
+  free(tmp);
+  if (energy) cudaMemcpy(energy, st->energy_d + (which == 0 ? eenb14 : eenbrecipexcl), sizeof(double),
+                         cudaMemcpyDeviceToHost);
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+

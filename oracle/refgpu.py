@@ -28,6 +28,8 @@ def lib():
         L.ref_evaluate.argtypes = [p, i, i, p, p, p]
         L.ref_time.argtypes = [p, p, i, i, i, p, C.c_size_t, p]
         L.ref_list_info.argtypes = [p, p, p]
+        L.ref_set_pairs.argtypes = [p, i, p, i, p, i]
+        L.ref_evaluate_pairs.argtypes = [p, i, i, p, p, p]
         _lib = L
     return _lib
 
@@ -71,6 +73,28 @@ class RefGPU:
                                 e.ctypes.data_as(C.c_void_p), lf.ctypes.data_as(C.c_void_p))
         if rc != 0:
             raise RuntimeError("reference harness: evaluate failed")
+        return {"grad": g.reshape(-1, 3), "energy": float(e[0]), "lambdaForce": lf}
+
+    def set_pairs(self, soft14=False):
+        """The system's nb14 / nbex lists (NB14_DTYPE / NBEX_DTYPE, the reference's layouts)."""
+        from blade_b200.systems import NB14_DTYPE, NBEX_DTYPE
+        self._p14 = np.ascontiguousarray(self.sys.nb14 if self.sys.nb14 is not None else np.zeros(0, NB14_DTYPE))
+        self._pex = np.ascontiguousarray(self.sys.nbex if self.sys.nbex is not None else np.zeros(0, NBEX_DTYPE))
+        rc = lib().ref_set_pairs(self.h, len(self._p14), self._p14.ctypes.data_as(C.c_void_p), len(self._pex),
+                                 self._pex.ctypes.data_as(C.c_void_p), int(bool(soft14)))
+        if rc != 0:
+            raise RuntimeError("reference harness: set_pairs failed")
+
+    def evaluate_pairs(self, which="nb14", xyz=None, lam=None, energy=True):
+        """getforce_nb14 / getforce_nbex of the reference on the given state."""
+        self.set_state(self.sys.xyz if xyz is None else xyz, self.sys.lambdas() if lam is None else lam)
+        g = np.zeros(3 * self.N)
+        e = np.zeros(1)
+        lf = np.zeros(self.nL)
+        rc = lib().ref_evaluate_pairs(self.h, 0 if which == "nb14" else 1, int(energy), g.ctypes.data_as(C.c_void_p),
+                                      e.ctypes.data_as(C.c_void_p), lf.ctypes.data_as(C.c_void_p))
+        if rc != 0:
+            raise RuntimeError("reference harness: evaluate_pairs failed")
         return {"grad": g.reshape(-1, 3), "energy": float(e[0]), "lambdaForce": lf}
 
     def time(self, frames_d, steps, rebuild_every=10, energy_every=10, flush=None):

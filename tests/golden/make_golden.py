@@ -5,11 +5,14 @@ unmodified, built into oracle/_ref/libbladeref.so by oracle/ref/Makefile) on
 the seeded synthetic systems and stores coordinates, FP32 forces (dU/dx),
 dU/dlambda and the nbdirect energy.  Needs a GPU:
 
-    python tests/golden/make_golden.py OUTDIR
+    python tests/golden/make_golden.py OUTDIR [--pairs-only]
 
 Cases: the 216-water box under all nine elecMethod x vdwMethod combinations,
 the MSLD water box (soft core on and off), and the 23,558-atom chain-in-water
-system (forces of the first 3,000 atoms kept).
+system (forces of the first 3,000 atoms kept); and, from the reference's
+getforce_nb14 / getforce_nbex (src/bonded/pair.cu), pairs_*.npz for a small
+chain-in-water system (1-4 pairs with e14fac 0.5 under three method
+combinations, PME exclusion corrections) and the MSLD water box.
 """
 import os
 import sys
@@ -36,9 +39,24 @@ def cases():
     yield "chain_water_23558", systems.chain_in_water(), 3000
 
 
-def main(out):
+def pair_cases():
+    """(name, system, which, soft14, atoms kept) of the nb14 / nbex fixtures."""
+    base = systems.chain_in_water(seed=5, box=30.0, n_chain=250, n_wat=780, name="chain_water_small")
+    for e, v in ((1, 0), (0, 1), (2, 2)):
+        s = systems.with_pair_lists(base, e14fac=0.5)
+        s.elecMethod, s.vdwMethod = e, v
+        yield f"pairs_nb14_e{e}v{v}", s, "nb14", False, 400
+    s = systems.with_pair_lists(base, e14fac=0.5)
+    yield "pairs_nbex", s, "nbex", False, None
+    m = systems.with_pair_lists(systems.msld_water())
+    yield "pairs_msld_nb14_soft", m, "nb14", True, None
+    yield "pairs_msld_nb14_hard", m, "nb14", False, None
+    yield "pairs_msld_nbex", m, "nbex", False, None
+
+
+def main(out, pairs_only=False):
     os.makedirs(out, exist_ok=True)
-    for name, s, keep in cases():
+    for name, s, keep in ([] if pairs_only else cases()):
         r = refgpu.RefGPU(s).evaluate()
         g = r["grad"].astype(np.float32)
         n = s.N if keep is None else keep
@@ -47,7 +65,18 @@ def main(out):
                             lambdaForce=r["lambdaForce"].astype(np.float64), n_forces=np.int64(n),
                             elecMethod=np.int64(s.elecMethod), vdwMethod=np.int64(s.vdwMethod))
         print(name, s.N, r["energy"], flush=True)
+    for name, s, which, soft, keep in pair_cases():
+        ref = refgpu.RefGPU(s)
+        ref.set_pairs(soft)
+        r = ref.evaluate_pairs(which)
+        n = s.N if keep is None else keep
+        np.savez_compressed(os.path.join(out, name + ".npz"), xyz=s.xyz.astype(np.float32),
+                            grad=r["grad"].astype(np.float32)[:n], energy=np.float64(r["energy"]),
+                            lambdaForce=r["lambdaForce"].astype(np.float64), n_forces=np.int64(n),
+                            elecMethod=np.int64(s.elecMethod), vdwMethod=np.int64(s.vdwMethod))
+        print(name, which, len(s.nb14), len(s.nbex), r["energy"], flush=True)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "golden_out"))
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    main(args[0] if args else os.path.join(ROOT, "golden_out"), pairs_only="--pairs-only" in sys.argv)
