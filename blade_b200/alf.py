@@ -528,11 +528,13 @@ def site_iterations_to_flat(recs_dev_frac) -> np.ndarray:
     return first
 
 
-def run_sites(drv: AlfBatch, n_iter: int, model=None, scale: float = 1.0, with_plain: bool = False):
+def run_sites(drv: AlfBatch, n_iter: int, model=None, scale: float = 1.0, with_plain: bool = False,
+              learned_iters: int | None = None):
     """n_iter iterations of plain (model None) or learned flattening; returns
     per-iteration records with per-site flatness and whether the plain
     fallback was used.  The learned step is ``scale`` times the predicted
-    lookahead change, added to the plain update when ``with_plain``."""
+    lookahead change, added to the plain update when ``with_plain``; with
+    ``learned_iters`` only the first that many iterations use the network."""
     import torch
     R = drv.sm.n_replicas
     prev = np.full(R, np.inf)
@@ -545,7 +547,7 @@ def run_sites(drv: AlfBatch, n_iter: int, model=None, scale: float = 1.0, with_p
         plain = plain_update(drv.sm, h1, h2, he, drv.T)
         rec = {"params": drv.params.copy(), "h1": h1, "h2": h2, "he": he, "site_dev": sdev, "site_frac": sfrac,
                "fallback": None}
-        if model is None:
+        if model is None or (learned_iters is not None and it >= learned_iters):
             delta = plain
         else:
             X = torch.from_numpy(replica_features(drv.sm, h1, h2, drv.params)).to(drv.B.dev)

@@ -289,7 +289,7 @@ struct JRegs {
 template <int ELEC, int VDW, bool ENERGY, bool COMBINE, bool MASKED, int ALCH>
 __device__ __forceinline__ void plain_loop(JRegs<COMBINE, ALCH> &J, const float4 &xi, uint32_t row, int gj,
                                            int rot, const PairConst &pc, const float2 *sLJ, int rowI,
-                                           float2 ljI, float &fix, float &fiy, float &fiz, float &ei,
+                                           float2 ljI, float &fix, float &fiy, float &fiz, long long &ei,
                                            unsigned long long &pairs, int count) {
 #pragma unroll 4
   for (int k = 0; k < gj; k++) {
@@ -313,7 +313,7 @@ __device__ __forceinline__ void plain_loop(JRegs<COMBINE, ALCH> &J, const float4
                                                               ljI, make_float2(J.ex, J.er), E);
       fix = fmaf(fs, dx, fix); fiy = fmaf(fs, dy, fiy); fiz = fmaf(fs, dz, fiz);
       J.fx = fmaf(-fs, dx, J.fx); J.fy = fmaf(-fs, dy, J.fy); J.fz = fmaf(-fs, dz, J.fz);
-      ei += E;
+      ei += to_fix(E);  // energies in fixed point per pair: exact sums of the FP32 pair values
       if (count) pairs++;
     }
     J.move(rot, gj, MASKED || !COMBINE, false);
@@ -396,7 +396,8 @@ __global__ void __launch_bounds__(256, ALCH ? 3 : 4) k_pair(KArgs A) {
     }
     unsigned act = __ballot_sync(kFull, hit);
 
-    float fix = 0.f, fiy = 0.f, fiz = 0.f, ei = 0.f, fli = 0.f;
+    float fix = 0.f, fiy = 0.f, fiz = 0.f, fli = 0.f;
+    long long ei = 0;  // fixed-point energy of this lane's pairs
     while (act) {
       const int c = __ffs(act) - 1;
       act &= act - 1;
@@ -512,7 +513,7 @@ __global__ void __launch_bounds__(256, ALCH ? 3 : 4) k_pair(KArgs A) {
             const float fs = dEdr * dredr * rinv;
             fix = fmaf(fs, dx, fix); fiy = fmaf(fs, dy, fiy); fiz = fmaf(fs, dz, fiz);
             J.fx = fmaf(-fs, dx, J.fx); J.fy = fmaf(-fs, dy, J.fy); J.fz = fmaf(-fs, dz, J.fz);
-            if (ENERGY) ei = fmaf(s, E, ei);
+            if (ENERGY) ei += to_fix(s * E);
             if (ENERGY && A.count) pairs++;
           }
           J.move(rot, gj);
@@ -556,7 +557,7 @@ __global__ void __launch_bounds__(256, ALCH ? 3 : 4) k_pair(KArgs A) {
       atomicAdd(reinterpret_cast<unsigned long long *>(&sAccL[bi & 0xFFFF]),
                 static_cast<unsigned long long>(to_fix(fli)));
     if (ENERGY) {
-      long long e = to_fix(ei);
+      long long e = ei;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(kFull, e, o);
       if (lane == 0 && e != 0) red_add(&d.accE[d.blockRep[iBlock]], e);

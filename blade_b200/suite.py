@@ -281,11 +281,13 @@ def run_alf(args):
     reps = flattening_replicas(range(50000, 50000 + R))
     out = {}
     modes = [m for m in args.eval_modes.split(",") if m]
-    for name in modes:                                  # plain | learned:<scale> | plain+learned:<scale>
+    for name in modes:  # plain | learned:<scale> | plain+learned:<scale> | learned_first:<iterations>
         mdl = None if name == "plain" else model
-        scale = float(name.split(":")[1]) if ":" in name else 1.0
+        arg = float(name.split(":")[1]) if ":" in name else 1.0
+        first = int(arg) if name.startswith("learned_first") else None
         drv = alf.AlfBatch(reps, steps=K, seed=99)
-        recs = alf.run_sites(drv, args.eval_iters, mdl, scale=scale, with_plain=name.startswith("plain+"))
+        recs = alf.run_sites(drv, args.eval_iters, mdl, scale=1.0 if first is not None else arg,
+                             with_plain=name.startswith("plain+"), learned_iters=first)
         st = drv.status()
         drv.close()
         itf = alf.site_iterations_to_flat([(r["site_dev"], r["site_frac"]) for r in recs])
