@@ -14,6 +14,7 @@
 namespace bnb {
 
 constexpr int kNumShifts = 14;        // own image + 13 half-shell images
+constexpr int kExclBlk = 16;          // exclusion-partner blocks listed per block
 constexpr int kTilesPerWork = 8;      // default candidate tiles per pair-kernel work item
 constexpr int kMinTilesPerWork = 4;   // smallest setting (sizes the work-item capacity)
 constexpr int kMaxTableTypes = 64;    // LJ table kept in shared memory up to 64 types
@@ -87,6 +88,9 @@ struct Dev {
   float *slotQ;            // [32*maxBlocks]
   int *slotType;           // [32*maxBlocks]
   int *slotSiteBlock;      // [32*maxBlocks]
+  float4 *colMin, *colMax; // [totalCols] union of the column's block AABBs (cull pre-test)
+  int *exclBlk;            // [maxBlocks*kExclBlk] distinct blocks holding excluded partners
+  int *exclBlkCount;       // [maxBlocks] entries in exclBlk, -1 = more than kExclBlk
   int *cullCount;          // [maxBlocks*kNumShifts]
   int *cullOffset;         // [maxBlocks*kNumShifts+1]
   int4 *cand;              // [capCand] (jBlock, shiftCode, maskIdx, iBlock)

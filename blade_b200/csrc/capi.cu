@@ -163,6 +163,8 @@ int alloc_list(bnb_handle *h) {
   size_t o_bb = a.take<int>(MB + 1), o_brep = a.take<int>(MB), o_rbs = a.take<int>(h->R + 1);
   size_t o_slotA = a.take<int>(32 * MB), o_atomSlot = a.take<int>(N), o_slotQ = a.take<float>(32 * MB),
          o_slotT = a.take<int>(32 * MB), o_slotSB = a.take<int>(32 * MB);
+  size_t o_cmin = a.take<float4>(C), o_cmax = a.take<float4>(C), o_eb = a.take<int>(bnb::kExclBlk * MB),
+         o_ebc = a.take<int>(MB);
   size_t o_cullC = a.take<int>(MB * bnb::kNumShifts), o_cullO = a.take<int>(MB * bnb::kNumShifts + 1);
   size_t o_cand = a.take<int4>(h->capCand), o_cflag = a.take<int>(h->capCand),
          o_cmo = a.take<int>(h->capCand + 1);
@@ -195,6 +197,10 @@ int alloc_list(bnb_handle *h) {
   d.slotQ = (float *)(b + o_slotQ);
   d.slotType = (int *)(b + o_slotT);
   d.slotSiteBlock = (int *)(b + o_slotSB);
+  d.colMin = (float4 *)(b + o_cmin);
+  d.colMax = (float4 *)(b + o_cmax);
+  d.exclBlk = (int *)(b + o_eb);
+  d.exclBlkCount = (int *)(b + o_ebc);
   d.cullCount = (int *)(b + o_cullC);
   d.cullOffset = (int *)(b + o_cullO);
   d.cand = (int4 *)(b + o_cand);

@@ -391,7 +391,45 @@ __global__ void k_pack(Dev d, const float *__restrict__ pos) {
 
 namespace {
 
+// 6b. Column AABBs: union of the AABBs of each column's blocks (one warp per
+//     column).  The union contains every member box, so with the rounding of
+//     aabb_hit a block that hits implies its column hits; the cull below may
+//     skip columns that miss without changing the candidate list.
+__global__ void k_colbox(Dev d) {
+  const int lane = threadIdx.x & 31;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  const int B = d.ctr->blockCount;
+  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < d.totalCols; c += nWarps) {
+    int b0 = d.colStartBlock[c], b1 = d.colStartBlock[c + 1];
+    b1 = b1 < B ? b1 : B;
+    float3 mn = make_float3(INFINITY, INFINITY, INFINITY), mx = make_float3(-INFINITY, -INFINITY, -INFINITY);
+    for (int b = b0 + lane; b < b1; b += 32) {
+      const float4 lo = d.bmin[b], hi = d.bmax[b];
+      mn.x = fminf(mn.x, lo.x); mn.y = fminf(mn.y, lo.y); mn.z = fminf(mn.z, lo.z);
+      mx.x = fmaxf(mx.x, hi.x); mx.y = fmaxf(mx.y, hi.y); mx.z = fmaxf(mx.z, hi.z);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mn.x = fminf(mn.x, __shfl_xor_sync(kFull, mn.x, o));
+      mn.y = fminf(mn.y, __shfl_xor_sync(kFull, mn.y, o));
+      mn.z = fminf(mn.z, __shfl_xor_sync(kFull, mn.z, o));
+      mx.x = fmaxf(mx.x, __shfl_xor_sync(kFull, mx.x, o));
+      mx.y = fmaxf(mx.y, __shfl_xor_sync(kFull, mx.y, o));
+      mx.z = fmaxf(mx.z, __shfl_xor_sync(kFull, mx.z, o));
+    }
+    if (lane == 0) {
+      d.colMin[c] = make_float4(mn.x, mn.y, mn.z, 0.f);
+      d.colMax[c] = make_float4(mx.x, mx.y, mx.z, 0.f);
+    }
+  }
+}
+
 // 7/9. Cull: one warp per (iBlock, shift code); count pass then write pass.
+//      The j blocks of the replica are visited column by column: lanes test
+//      32 columns' AABBs at once, the blocks of the columns that hit are
+//      concatenated (warp scan of their counts) and tested 32 at a time.
+//      Columns and the blocks inside them are in increasing block order, so
+//      the candidates come out in the order of a scan over all j blocks.
 template <bool kWrite>
 __global__ void k_cull(Dev d, float rcull2) {
   const int lane = threadIdx.x & 31;
@@ -410,20 +448,50 @@ __global__ void k_cull(Dev d, float rcull2) {
     float3 sh = make_float3(__fmul_rn((float)sx, ri.box[0]), __fmul_rn((float)sy, ri.box[1]),
                             __fmul_rn((float)sz, ri.box[2]));
     float4 imin = d.bmin[iBlock], imax = d.bmax[iBlock];
-    int j0 = code == 0 ? iBlock : d.repBlockStart[r];
-    int j1 = d.repBlockStart[r + 1];
+    const int j0 = code == 0 ? iBlock : d.repBlockStart[r];
+    const int j1 = d.repBlockStart[r + 1];
     int cnt = 0;
     int base = kWrite ? d.cullOffset[gw] : 0;
-    for (int jb = j0; jb < j1; jb += 32) {
-      int j = jb + lane;
-      bool hit = false;
-      if (j < j1) hit = aabb_hit(imin, imax, d.bmin[j], d.bmax[j], sh, rcull2);
-      unsigned m = __ballot_sync(kFull, hit);
-      if (kWrite && hit) {
-        int p = base + cnt + __popc(m & ((1u << lane) - 1u));
-        if (p < d.capCand) d.cand[p] = make_int4(j, code, -1, iBlock);
+    for (int cb = 0; cb < ri.nCols; cb += 32) {
+      const int c = ri.colStart + cb + lane;
+      int bs = 0, n = 0;
+      if (cb + lane < ri.nCols) {
+        bs = d.colStartBlock[c];
+        int be = d.colStartBlock[c + 1];
+        bs = bs > j0 ? bs : j0;
+        be = be < j1 ? be : j1;
+        if (bs < be && aabb_hit(imin, imax, d.colMin[c], d.colMax[c], sh, rcull2)) n = be - bs;
       }
-      cnt += __popc(m);
+      int inc = n;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, inc, o);
+        if (lane >= o) inc += y;
+      }
+      const int tot = __shfl_sync(kFull, inc, 31);
+      const int exc = inc - n;
+      for (int t0 = 0; t0 < tot; t0 += 32) {
+        const int t = t0 + lane;
+        // column lane k holding item t: the first lane whose inclusive count exceeds t
+        int k = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1)
+          if (__shfl_sync(kFull, inc, k + step - 1) <= t) k += step;
+        const int jStart = __shfl_sync(kFull, bs, k);
+        const int jOff = __shfl_sync(kFull, exc, k);
+        bool hit = false;
+        if (t < tot) {
+          const int j = jStart + (t - jOff);
+          hit = aabb_hit(imin, imax, d.bmin[j], d.bmax[j], sh, rcull2);
+        }
+        const unsigned m = __ballot_sync(kFull, hit);
+        if (kWrite && hit) {
+          const int j = jStart + (t - jOff);
+          int p = base + cnt + __popc(m & ((1u << lane) - 1u));
+          if (p < d.capCand) d.cand[p] = make_int4(j, code, -1, iBlock);
+        }
+        cnt += __popc(m);
+      }
     }
     if (!kWrite && lane == 0) d.cullCount[gw] = cnt;
   }
@@ -467,6 +535,50 @@ __device__ __forceinline__ uint32_t excl_row(const Dev &d, int iBlock, int jBloc
   return row;
 }
 
+// 10a. Exclusion-partner blocks: per block, the distinct blocks that hold an
+//      excluded partner of one of its atoms (one warp per block, lane = atom).
+//      Candidate tiles whose j block is not listed carry no exclusion, so
+//      k_excl skips their per-atom scan.  More than kExclBlk blocks: count -1,
+//      and every tile of the block takes the full scan.
+__global__ void k_excl_blocks(Dev d) {
+  __shared__ int sList[8][kExclBlk];
+  const int lane = threadIdx.x & 31;
+  const int warp = (threadIdx.x >> 5) & 7;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  const int B = d.ctr->blockCount;
+  for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < B; b += nWarps) {
+    const int a = d.slotAtom[32 * b + lane];
+    int e = 0, e1 = 0;
+    if (a >= 0) {
+      e = d.exclStart[a];
+      e1 = d.exclStart[a + 1];
+    }
+    int n = 0;       // blocks listed so far (warp-uniform)
+    int mine = -1;   // lane k < n holds the k-th listed block
+    while (__any_sync(kFull, e < e1) && n <= kExclBlk) {
+      int jb = -1;
+      if (e < e1) {
+        const int p = d.exclAtom[e++];
+        if (p != a) jb = d.atomSlot[p] >> 5;
+      }
+      const int listed = n < kExclBlk ? n : kExclBlk;
+      for (int k = 0; k < listed; k++)
+        if (jb == __shfl_sync(kFull, mine, k)) jb = -1;
+      const unsigned grp = __match_any_sync(kFull, jb);
+      const bool lead = jb >= 0 && (__ffs(grp) - 1) == lane;
+      const unsigned leaders = __ballot_sync(kFull, lead);
+      const int pos = n + __popc(leaders & ((1u << lane) - 1u));
+      if (lead && pos < kExclBlk) sList[warp][pos] = jb;
+      n += __popc(leaders);
+      __syncwarp();
+      mine = lane < (n < kExclBlk ? n : kExclBlk) ? sList[warp][lane] : -1;
+      __syncwarp();
+    }
+    if (lane < kExclBlk) d.exclBlk[kExclBlk * b + lane] = mine;
+    if (lane == 0) d.exclBlkCount[b] = n <= kExclBlk ? n : -1;
+  }
+}
+
 template <bool kWrite>
 __global__ void k_excl(Dev d) {
   const int lane = threadIdx.x & 31;
@@ -478,7 +590,13 @@ __global__ void k_excl(Dev d) {
       continue;
     }
     int4 t = d.cand[c];
-    uint32_t row = excl_row(d, t.w, t.x, lane);
+    const int nb = d.exclBlkCount[t.w];
+    bool scan = true;
+    if (nb >= 0) {
+      const int v = lane < nb ? d.exclBlk[kExclBlk * t.w + lane] : -1;
+      scan = __any_sync(kFull, v == t.x);
+    }
+    uint32_t row = scan ? excl_row(d, t.w, t.x, lane) : 0xFFFFFFFFu;
     bool any = __any_sync(kFull, row != 0xFFFFFFFFu);
     if (!kWrite) {
       if (lane == 0) d.candFlag[c] = any ? 1 : 0;
@@ -534,13 +652,15 @@ void pack_positions(const Dev &d, const float *pos, cudaStream_t s) {
 int rebuild_list(const Dev &d, const int *colRep, const float *pos, float rcull2,
                  cudaStream_t s) {
   cudaMemsetAsync(d.colCount, 0, sizeof(int) * d.totalCols, s);
-  const int launches = (d.N > 0 ? 2 : 0) + 20;
+  const int launches = (d.N > 0 ? 2 : 0) + 22;
   if (d.N > 0) k_bin<<<grid_for(d.N, 256), 256, 0, s>>>(d, pos);
   k_colscan<<<1, 1024, 0, s>>>(d, colRep);
   if (d.N > 0) k_scatter<<<grid_for(d.N, 256), 256, 0, s>>>(d);
   k_colsort<<<d.totalCols, 512, 0, s>>>(d);
   k_slots<<<grid_for(32LL * d.maxBlocks, 256), 256, 0, s>>>(d);
   pack_positions(d, pos, s);
+  k_colbox<<<grid_for(32LL * d.totalCols, 256), 256, 0, s>>>(d);
+  k_excl_blocks<<<grid_for(32LL * d.maxBlocks, 256), 256, 0, s>>>(d);
   // cull: count, scan, write
   const int cullWarps = d.maxBlocks * kNumShifts;
   const int cullGrid = grid_for(32LL * cullWarps, 256) < 148 * 32 ? grid_for(32LL * cullWarps, 256) : 148 * 32;

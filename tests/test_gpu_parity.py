@@ -95,8 +95,23 @@ def test_unwrapped_coordinates(cuda):
     check(s2, run(s2), oracle.nbdirect(s2))
 
 
+def _wide_exclusions():
+    """Water box whose first 8 atoms are each excluded with 40 atoms spread
+    over the box: their blocks list more than 16 exclusion-partner blocks, so
+    the builder's per-block partner list overflows and takes the full scan."""
+    s = systems.water_box()
+    rng = np.random.default_rng(8)
+    extra = []
+    for a in range(8):
+        for b in rng.choice(np.arange(8, s.N), 40, replace=False):
+            extra += [(a, int(b)), (int(b), a)]
+    s.excl = np.unique(np.concatenate([s.excl, np.int32(extra)]), axis=0).astype(np.int32)
+    s.name = "water_wide_excl"
+    return s
+
+
 def test_list_bitexact_against_oracle(cuda):
-    for s in (systems.water_box(), systems.msld_water(),
+    for s in (systems.water_box(), systems.msld_water(), _wide_exclusions(),
               systems.chain_in_water(seed=5, box=40.0, n_chain=600, n_wat=1800, name="chain_small")):
         nb = NbDirect(s)
         pos = nb.positions_tensor()
