@@ -75,6 +75,10 @@ def lib():
             "bnb_compute_nb14": (i, [p, p, p, p, i, p, p]),
             "bnb_compute_nbex": (i, [p, p, p, p, i, p, p]),
             "bnb_nbdirect_noalloc": (i, [p, i, p, p, p, i, p, p, p, i, p, p]),
+            "bnb_set_pme": (i, [p, i, f, p, p]),
+            "bnb_pme_grid": (i, [p, i, p]),
+            "bnb_compute_pme": (i, [p, p, p, p, i, p, p]),
+            "bnb_compute_ewald_self": (i, [p, p, i, p, p]),
             "bnb_mlp_linear_forward": (i, [i, i, i, p, p, p, i, p, p, p, p]),
             "bnb_mlp_linear_backward": (i, [i, i, i, p, p, i, p, p, p, p, p, p, p, p]),
             "bnb_mlp_mse": (i, [i, i, p, p, p, p, p, p, p]),

@@ -7,6 +7,7 @@
 // two arenas (topology, list); capacities grow only inside a synchronous
 // rebuild, never during an asynchronous (graph-capturable) call.
 #include <cuda_runtime.h>
+#include <cufft.h>
 
 #include <algorithm>
 #include <cmath>
@@ -14,6 +15,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <tuple>
 #include <vector>
 
 #include "bnb.h"
@@ -22,6 +24,7 @@
 #include "listbuild.h"
 #include "nbdirect.h"
 #include "pairs.h"
+#include "pme.h"
 
 using bnb::Dev;
 using bnb::PairConst;
@@ -68,6 +71,16 @@ struct bnb_handle {
   bnb_nb14 *nb14_d = nullptr;
   bnb_nbex *nbex_d = nullptr;
   long long *accP = nullptr, *accPL = nullptr, *accPE = nullptr;
+  // PME reciprocal space (bnb_set_pme)
+  void *pmeArena = nullptr;
+  int pmeOrder = 0, pmeTotalGrid = 0, pmeTotalCplx = 0, pmeMaxCplx = 0;
+  std::vector<bnb::PmeRep> pmeRep;
+  struct PmePlan { cufftHandle r2c, c2r; int first, count; };
+  std::vector<PmePlan> pmePlans;
+  bnb::PmeRep *pmeRep_d = nullptr;
+  float *pmeMod_d = nullptr, *pmeGrid_d = nullptr;
+  float2 *pmeCplx_d = nullptr;
+  long long *pmeFix_d = nullptr, *pmeAccL = nullptr, *pmeAccE = nullptr;
 };
 
 namespace {
@@ -141,6 +154,18 @@ PairConst make_const(const bnb_params &p) {
   c.vshRc12inv = (float)(1.0 / (rc6 * rc6));
   c.vshRc18inv = (float)(1.0 / (rc6 * rc6 * rc6));
   return c;
+}
+
+void free_pme(bnb_handle *h) {
+  for (auto &p : h->pmePlans) {
+    cufftDestroy(p.r2c);
+    cufftDestroy(p.c2r);
+  }
+  h->pmePlans.clear();
+  if (h->pmeArena) cudaFree(h->pmeArena);
+  h->pmeArena = nullptr;
+  h->pmeOrder = 0;
+  h->pmeRep.clear();
 }
 
 void free_list(bnb_handle *h) {
@@ -356,6 +381,7 @@ int bnb_destroy(bnb_handle *h) {
   free_list(h);
   if (h->topoArena) cudaFree(h->topoArena);
   if (h->pairArena) cudaFree(h->pairArena);
+  free_pme(h);
   destroy_events(h);
   delete h;
   return BNB_OK;
@@ -1062,3 +1088,212 @@ extern "C" int bnb_compute_nbex(bnb_handle *h, const float *position, const floa
   return bnb::launch_nbex(a, *out, calcEnergy != 0, s);
 }
 
+
+// ---------------------------------------------------------------------------
+// PME reciprocal space and Ewald self term (getforce_ewald /
+// getforce_ewaldself, src/nbrecip/nbrecip.cu:19-555); grid sizes and B-spline
+// moduli as Potential::initialize (src/system/potential.cxx:1202-1300).
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kPmePad = 64;  // grid offsets in multiples of 64 elements
+
+// The reference's grid rule: the smallest of j*{32,27,24,20,18} above
+// L/spacing, with j the power of two that puts L/spacing in [16j, 32j).
+int pme_grid_size(float L, float spacing) {
+  static const int good[] = {32, 27, 24, 20, 18, 16};
+  const float md = L / spacing;
+  int j = 1;
+  while (md >= 32.0f * j) j *= 2;
+  int k = 0;
+  while (k < 5 && md < (float)(j * good[k])) k++;
+  return j * good[k - 1];
+}
+
+// 1/|b(m)|^2, b(m) = sum_{l=1}^{n-1} M_n(l) exp(2 pi i m l / K), m = 0..count-1.
+void pme_moduli(int K, int order, int count, float *out) {
+  double M[12] = {0};
+  M[1] = 1.0;  // M_2 at the integers 0, 1, 2
+  for (int k = 3; k <= order; k++) {
+    double nw[12] = {0};
+    for (int l = 0; l <= k; l++) nw[l] = (l * M[l] + (k - l) * (l >= 1 ? M[l - 1] : 0.0)) / (k - 1);
+    for (int l = 0; l < 12; l++) M[l] = nw[l];
+  }
+  const double tau = 6.283185307179586476925;
+  for (int m = 0; m < count; m++) {
+    double re = 0.0, im = 0.0;
+    for (int l = 1; l < order; l++) {
+      re += M[l] * std::cos(tau * m * l / K);
+      im += M[l] * std::sin(tau * m * l / K);
+    }
+    out[m] = (float)(1.0 / (re * re + im * im));
+  }
+}
+
+inline long long pad_to(long long n) { return (n + kPmePad - 1) / kPmePad * kPmePad; }
+
+bnb::PmeArgs pme_args(bnb_handle *h, const float *position, const float *lambda) {
+  bnb::PmeArgs a{};
+  a.N = h->N;
+  a.R = h->R;
+  a.lamTotal = h->lamTotal;
+  a.order = h->pmeOrder;
+  a.totalGrid = h->pmeTotalGrid;
+  a.totalCplx = h->pmeTotalCplx;
+  a.beta = h->p.betaEwald;
+  a.x = position;
+  a.lambda = lambda;
+  a.q = h->d.atomQ;
+  a.siteBlock = h->d.atomSiteBlock;
+  a.atomRep = h->d.atomRep;
+  a.rep = h->d.rep;
+  a.prep = h->pmeRep_d;
+  a.maxCplx = h->pmeMaxCplx;
+  a.mod = h->pmeMod_d;
+  a.qfix = h->pmeFix_d;
+  a.grid = h->pmeGrid_d;
+  a.cplx = h->pmeCplx_d;
+  a.accL = h->pmeAccL;
+  a.accE = h->pmeAccE;
+  return a;
+}
+}  // namespace
+
+extern "C" int bnb_set_pme(bnb_handle *h, int order, float gridSpace, const int *grid, const float *boxes) {
+  if (!h || !boxes || (order != 4 && order != 6 && order != 8) || (!grid && !(gridSpace > 0.f)))
+    return BNB_ERR_ARG;
+  if (!h->topo) return BNB_ERR_STATE;
+  const int R = h->R;
+  std::vector<bnb::PmeRep> pr(R);
+  for (int r = 0; r < R; r++)
+    for (int k = 0; k < 3; k++) {
+      if (!(boxes[3 * r + k] > 0.f)) return BNB_ERR_ARG;
+      const int K = grid ? grid[3 * r + k] : pme_grid_size(boxes[3 * r + k], gridSpace);
+      if (K < order || K > 4096) return BNB_ERR_ARG;
+      pr[r].K[k] = K;
+    }
+  // Grids are laid out grouped by size (stable in replica order), so every
+  // set of equal grids is one batched FFT plan.
+  std::vector<int> layout(R);
+  for (int r = 0; r < R; r++) layout[r] = r;
+  auto key = [&](int r) { return std::make_tuple(pr[r].K[0], pr[r].K[1], pr[r].K[2]); };
+  std::stable_sort(layout.begin(), layout.end(), [&](int x, int y) { return key(x) < key(y); });
+  long long gOff = 0, cOff = 0, mOff = 0;
+  for (int r : layout) {
+    pr[r].gridOff = (int)gOff;
+    pr[r].cplxOff = (int)cOff;
+    pr[r].modOff = (int)mOff;
+    gOff += pad_to((long long)pr[r].K[0] * pr[r].K[1] * pr[r].K[2]);
+    cOff += pad_to((long long)pr[r].K[0] * pr[r].K[1] * (pr[r].K[2] / 2 + 1));
+    mOff += pr[r].K[0] + pr[r].K[1] + pr[r].K[2] / 2 + 1;
+    if (gOff > (1LL << 30) || cOff > (1LL << 30)) return BNB_ERR_TOO_LARGE;
+  }
+  free_pme(h);
+  Arena a;
+  size_t oRep = a.take<bnb::PmeRep>(std::max(R, 1)), oMod = a.take<float>(mOff), oFix = a.take<long long>(gOff),
+         oGrid = a.take<float>(gOff), oCplx = a.take<float2>(cOff), oL = a.take<long long>(std::max(h->lamTotal, 1)),
+         oE = a.take<long long>(std::max(R, 1));
+  void *base = nullptr;
+  if (!ok(cudaMalloc(&base, a.off))) return BNB_ERR_CUDA;
+  h->pmeArena = base;
+  char *b = static_cast<char *>(base);
+  h->pmeRep_d = (bnb::PmeRep *)(b + oRep);
+  h->pmeMod_d = (float *)(b + oMod);
+  h->pmeFix_d = (long long *)(b + oFix);
+  h->pmeGrid_d = (float *)(b + oGrid);
+  h->pmeCplx_d = (float2 *)(b + oCplx);
+  h->pmeAccL = (long long *)(b + oL);
+  h->pmeAccE = (long long *)(b + oE);
+  std::vector<float> mod(mOff);
+  for (int r = 0; r < R; r++) {
+    float *m = mod.data() + pr[r].modOff;
+    pme_moduli(pr[r].K[0], order, pr[r].K[0], m);
+    pme_moduli(pr[r].K[1], order, pr[r].K[1], m + pr[r].K[0]);
+    pme_moduli(pr[r].K[2], order, pr[r].K[2] / 2 + 1, m + pr[r].K[0] + pr[r].K[1]);
+  }
+  if (!ok(cudaMemset(base, 0, a.off)) ||
+      !ok(cudaMemcpy(h->pmeRep_d, pr.data(), sizeof(bnb::PmeRep) * R, cudaMemcpyHostToDevice)) ||
+      !ok(cudaMemcpy(h->pmeMod_d, mod.data(), sizeof(float) * mOff, cudaMemcpyHostToDevice))) {
+    free_pme(h);
+    return BNB_ERR_CUDA;
+  }
+  // one batched plan pair per set of equal grids (contiguous in the layout)
+  for (int i = 0; i < R;) {
+    const int r = layout[i];
+    int e = i + 1;
+    while (e < R && key(layout[e]) == key(r)) e++;
+    int n[3] = {pr[r].K[0], pr[r].K[1], pr[r].K[2]};
+    int nc[3] = {pr[r].K[0], pr[r].K[1], pr[r].K[2] / 2 + 1};
+    const int dr = (int)pad_to((long long)n[0] * n[1] * n[2]);
+    const int dc = (int)pad_to((long long)nc[0] * nc[1] * nc[2]);
+    bnb_handle::PmePlan p{};
+    p.first = r;
+    p.count = e - i;
+    if (cufftPlanMany(&p.r2c, 3, n, n, 1, dr, nc, 1, dc, CUFFT_R2C, p.count) != CUFFT_SUCCESS) {
+      free_pme(h);
+      return BNB_ERR_CUDA;
+    }
+    if (cufftPlanMany(&p.c2r, 3, n, nc, 1, dc, n, 1, dr, CUFFT_C2R, p.count) != CUFFT_SUCCESS) {
+      cufftDestroy(p.r2c);
+      free_pme(h);
+      return BNB_ERR_CUDA;
+    }
+    h->pmePlans.push_back(p);
+    i = e;
+  }
+  h->pmeRep = pr;
+  h->pmeOrder = order;
+  h->pmeTotalGrid = (int)gOff;
+  h->pmeTotalCplx = (int)cOff;
+  h->pmeMaxCplx = 0;
+  for (int r = 0; r < R; r++)
+    h->pmeMaxCplx = std::max(h->pmeMaxCplx, pr[r].K[0] * pr[r].K[1] * (pr[r].K[2] / 2 + 1));
+  return BNB_OK;
+}
+
+extern "C" int bnb_pme_grid(bnb_handle *h, int replica, int *K) {
+  if (!h || !K || replica < 0 || replica >= h->R) return BNB_ERR_ARG;
+  if (!h->pmeOrder) return BNB_ERR_STATE;
+  for (int k = 0; k < 3; k++) K[k] = h->pmeRep[replica].K[k];
+  return BNB_OK;
+}
+
+extern "C" int bnb_compute_pme(bnb_handle *h, const float *position, const float *lambda, const float *boxes,
+                               int calcEnergy, const bnb_outputs *out, void *stream) {
+  if (!h || !out || !boxes || (h->N > 0 && !position)) return BNB_ERR_ARG;
+  if (!h->pmeOrder) return BNB_ERR_STATE;
+  if (h->alch && !lambda) return BNB_ERR_ARG;
+  if (h->p.elecMethod != 1) return BNB_OK;  // reciprocal space exists for PME only (nbrecip.cu:486)
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = pairs_boxes(h, boxes, s);
+  if (rc) return rc;
+  bnb::PmeArgs a = pme_args(h, position, lambda);
+  if ((rc = bnb::pme_spread(a, s))) return rc;
+  for (auto &p : h->pmePlans) {
+    const bnb::PmeRep &f = h->pmeRep[p.first];
+    if (cufftSetStream(p.r2c, s) != CUFFT_SUCCESS ||
+        cufftExecR2C(p.r2c, h->pmeGrid_d + f.gridOff, reinterpret_cast<cufftComplex *>(h->pmeCplx_d + f.cplxOff)) !=
+            CUFFT_SUCCESS)
+      return BNB_ERR_CUDA;
+  }
+  if ((rc = bnb::pme_convolve(a, s))) return rc;
+  for (auto &p : h->pmePlans) {
+    const bnb::PmeRep &f = h->pmeRep[p.first];
+    if (cufftSetStream(p.c2r, s) != CUFFT_SUCCESS ||
+        cufftExecC2R(p.c2r, reinterpret_cast<cufftComplex *>(h->pmeCplx_d + f.cplxOff), h->pmeGrid_d + f.gridOff) !=
+            CUFFT_SUCCESS)
+      return BNB_ERR_CUDA;
+  }
+  h->launches += 5;
+  return bnb::pme_gather(a, *out, calcEnergy != 0, s);
+}
+
+extern "C" int bnb_compute_ewald_self(bnb_handle *h, const float *lambda, int calcEnergy, const bnb_outputs *out,
+                                      void *stream) {
+  if (!h || !out) return BNB_ERR_ARG;
+  if (!h->pmeOrder) return BNB_ERR_STATE;
+  if (h->alch && !lambda) return BNB_ERR_ARG;
+  if (h->p.elecMethod != 1) return BNB_OK;  // nbrecip.cu:64
+  bnb::PmeArgs a = pme_args(h, nullptr, lambda);
+  h->launches += 2;
+  return bnb::pme_self(a, *out, calcEnergy != 0, (cudaStream_t)stream);
+}

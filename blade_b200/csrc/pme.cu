@@ -1,0 +1,388 @@
+// PME reciprocal space and Ewald self term (sm_100a).
+//
+// Counterpart of getforce_ewald and getforce_ewaldself
+// (src/nbrecip/nbrecip.cu:19-555).  The algorithm is the reference's smooth
+// PME: lambda-scaled charges are spread with order-n cardinal B-splines
+// (grid point (floor(u) + t) mod K takes M_n(u - floor(u) + n - 1 - t),
+// u = x K / L; nbrecip.cu:85-213), the unnormalised R2C spectrum is
+// multiplied by B(m) exp(-pi^2 k^2 / beta^2) / (2 pi V k^2) (nbrecip.cu:
+// 215-256), the C2R result is the potential grid and the gather returns
+// dU/dx = 2 lambda q (K / L) sum dM M M phi, dU/dlambda = 2 q phi and
+// E = lambda q phi (nbrecip.cu:258-465).  Charges arrive scaled by
+// sqrt(kElectric), so the influence function carries no kElectric.
+// Differences by design:
+//   * the charge grid accumulates in int64 fixed point (2^-32), so the grid,
+//     and with it every output, is identical run to run;
+//   * u is formed in FP64 and wrapped with floor/mod, so any unwrapped
+//     coordinate lands on the right grid point;
+//   * lanes of an atom's 8-lane group own z offsets (contiguous grid
+//     addresses within one instruction) instead of x/y/z parity classes;
+//   * R replicas with their own grids in one launch per phase.
+// The 3-D FFTs are cuFFT plans (one batched plan per run of consecutive
+// replicas with equal grids), as in the reference.
+#include <cuda_runtime.h>
+
+#include "pme.h"
+
+namespace bnb {
+namespace {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr double kPi = 3.14159265358979323846;
+
+__device__ __forceinline__ long long to_fix(float v) { return __float2ll_rn(v * kFixScaleF); }
+
+__device__ __forceinline__ void red_add(long long *p, long long v) {
+  atomicAdd(reinterpret_cast<unsigned long long *>(p), static_cast<unsigned long long>(v));
+}
+
+// w[t] = M_n(f + n - 1 - t) and dw[t] = M_n'(f + n - 1 - t), t = 0..n-1, from
+// the Cox-de Boor recursion M_k(x) = (x M_{k-1}(x) + (k - x) M_{k-1}(x - 1))
+// / (k - 1) on the points x = f + j, and M_n'(x) = M_{n-1}(x) - M_{n-1}(x-1).
+template <int ORDER>
+__device__ __forceinline__ void bspline(float f, float (&w)[ORDER], float (&dw)[ORDER]) {
+  float a[ORDER];
+  float prev[ORDER];
+  a[0] = 1.f;
+#pragma unroll
+  for (int j = 1; j < ORDER; j++) a[j] = 0.f;
+#pragma unroll
+  for (int k = 2; k <= ORDER; k++) {
+    if (k == ORDER) {
+#pragma unroll
+      for (int j = 0; j < ORDER; j++) prev[j] = a[j];
+    }
+    const float inv = 1.f / (float)(k - 1);
+#pragma unroll
+    for (int j = k - 1; j >= 0; j--) {
+      const float x = f + (float)j;
+      const float left = j < k - 1 ? a[j] : 0.f;
+      const float right = j >= 1 ? a[j - 1] : 0.f;
+      a[j] = fmaf(x, left, ((float)k - x) * right) * inv;
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < ORDER; t++) {
+    const int j = ORDER - 1 - t;
+    w[t] = a[j];
+    dw[t] = (j < ORDER - 1 ? prev[j] : 0.f) - (j >= 1 ? prev[j - 1] : 0.f);
+  }
+}
+
+// Grid coordinate of one dimension: first grid index (mod K) and fraction.
+__device__ __forceinline__ void grid_coord(float x, int K, float L, int &i0, float &frac) {
+  const double u = (double)x * (double)K / (double)L;
+  const double u0 = floor(u);
+  frac = (float)(u - u0);
+  double m = u0 - (double)K * floor(u0 / (double)K);
+  i0 = (int)m;
+  if (i0 >= K) i0 -= K;  // m rounds to K only when u0 is a tiny negative multiple
+  if (i0 < 0) i0 += K;
+}
+
+__device__ __forceinline__ float atom_scale(const PmeArgs &a, int atom, int &block) {
+  block = a.siteBlock[atom] & 0xFFFF;
+  return (block && a.lambda) ? a.lambda[block] : 1.f;
+}
+
+// ---------------------------------------------------------------------------
+// Spread: 8 lanes per atom; lane g < ORDER owns z offset g and visits the
+// ORDER x ORDER (x, y) offsets.
+// ---------------------------------------------------------------------------
+template <int ORDER>
+__global__ void __launch_bounds__(256) k_spread(PmeArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int atom = t >> 3, g = t & 7;
+  if (atom >= a.N || g >= ORDER) return;
+  const int r = a.atomRep[atom];
+  const PmeRep pr = a.prep[r];
+  const RepInfo &ri = a.rep[r];
+  int block;
+  const float qe = a.q[atom] * atom_scale(a, atom, block);
+  if (qe == 0.f) return;
+  float wx[ORDER], wy[ORDER], wz[ORDER], d[ORDER];
+  int ix0, iy0, iz0;
+  float f;
+  grid_coord(a.x[3 * atom], pr.K[0], ri.box[0], ix0, f);
+  bspline<ORDER>(f, wx, d);
+  grid_coord(a.x[3 * atom + 1], pr.K[1], ri.box[1], iy0, f);
+  bspline<ORDER>(f, wy, d);
+  grid_coord(a.x[3 * atom + 2], pr.K[2], ri.box[2], iz0, f);
+  bspline<ORDER>(f, wz, d);
+  float wzg = wz[0];
+#pragma unroll
+  for (int k = 1; k < ORDER; k++) wzg = g == k ? wz[k] : wzg;
+  const float qz = qe * wzg;
+  int iz = iz0 + g;
+  if (iz >= pr.K[2]) iz -= pr.K[2];
+  long long *base = a.qfix + pr.gridOff;
+#pragma unroll
+  for (int tx = 0; tx < ORDER; tx++) {
+    int ix = ix0 + tx;
+    if (ix >= pr.K[0]) ix -= pr.K[0];
+    const float qx = qz * wx[tx];
+#pragma unroll
+    for (int ty = 0; ty < ORDER; ty++) {
+      int iy = iy0 + ty;
+      if (iy >= pr.K[1]) iy -= pr.K[1];
+      red_add(base + ((size_t)ix * pr.K[1] + iy) * pr.K[2] + iz, to_fix(qx * wy[ty]));
+    }
+  }
+}
+
+// Fixed point -> FP32 grid, clearing the fixed-point grid for the next call.
+__global__ void k_fix_to_grid(PmeArgs a) {
+  const double inv = 1.0 / kFixScale;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.totalGrid; i += gridDim.x * blockDim.x) {
+    const long long v = a.qfix[i];
+    a.grid[i] = (float)((double)v * inv);
+    if (v) a.qfix[i] = 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Convolution: blockIdx.y = replica, threads stride over its half spectrum.
+// FP32 like the reference's kernel (nbrecip.cu:215-256).
+// ---------------------------------------------------------------------------
+__global__ void k_convolve(PmeArgs a) {
+  const int r = blockIdx.y;
+  const PmeRep pr = a.prep[r];
+  const RepInfo &ri = a.rep[r];
+  const int K0 = pr.K[0], K1 = pr.K[1], K2h = pr.K[2] / 2 + 1;
+  const int n = K0 * K1 * K2h;
+  const float ix = 1.f / ri.box[0], iy = 1.f / ri.box[1], iz = 1.f / ri.box[2];
+  const float c = (float)(1.0 / (2.0 * kPi * (double)ri.box[0] * (double)ri.box[1] * (double)ri.box[2]));
+  const float g = (float)(kPi * kPi / ((double)a.beta * (double)a.beta));
+  const float *m0 = a.mod + pr.modOff, *m1 = m0 + K0, *m2 = m1 + K1;
+  float2 *spec = a.cplx + pr.cplxOff;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const int k = e % K2h;
+    const int row = e / K2h;
+    const int j = row % K1;
+    const int i = row / K1;
+    const float kx = (float)(2 * i <= K0 ? i : i - K0) * ix;
+    const float ky = (float)(2 * j <= K1 ? j : j - K1) * iy;
+    const float kz = (float)k * iz;
+    const float k2 = fmaf(kx, kx, fmaf(ky, ky, kz * kz));
+    const float factor = e == 0 ? 0.f : m0[i] * m1[j] * m2[k] * c * expf(-g * k2) / k2;
+    float2 v = spec[e];
+    v.x *= factor;
+    v.y *= factor;
+    spec[e] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Gather: same lane layout as the spread; the 8 lanes of an atom reduce with
+// xor shuffles, lane 0 of the group writes the atom's outputs.
+// ---------------------------------------------------------------------------
+template <int ORDER, bool ENERGY>
+__global__ void __launch_bounds__(256) k_gather(PmeArgs a, bnb_outputs o) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int atom = t >> 3, g = t & 7;
+  const bool valid = atom < a.N;
+  float phi = 0.f, gx = 0.f, gy = 0.f, gz = 0.f, qe = 0.f, qraw = 0.f;
+  int r = 0, block = 0;
+  PmeRep pr{};
+  if (valid) {
+    r = a.atomRep[atom];
+    pr = a.prep[r];
+    const RepInfo &ri = a.rep[r];
+    qraw = a.q[atom];
+    qe = qraw * atom_scale(a, atom, block);
+    if (g < ORDER) {
+      float wx[ORDER], wy[ORDER], wz[ORDER], dx[ORDER], dy[ORDER], dz[ORDER];
+      int ix0, iy0, iz0;
+      float f;
+      grid_coord(a.x[3 * atom], pr.K[0], ri.box[0], ix0, f);
+      bspline<ORDER>(f, wx, dx);
+      grid_coord(a.x[3 * atom + 1], pr.K[1], ri.box[1], iy0, f);
+      bspline<ORDER>(f, wy, dy);
+      grid_coord(a.x[3 * atom + 2], pr.K[2], ri.box[2], iz0, f);
+      bspline<ORDER>(f, wz, dz);
+      float wzg = wz[0], dzg = dz[0];
+#pragma unroll
+      for (int k = 1; k < ORDER; k++) {
+        wzg = g == k ? wz[k] : wzg;
+        dzg = g == k ? dz[k] : dzg;
+      }
+      int iz = iz0 + g;
+      if (iz >= pr.K[2]) iz -= pr.K[2];
+      const float *base = a.grid + pr.gridOff;
+#pragma unroll
+      for (int tx = 0; tx < ORDER; tx++) {
+        int ix = ix0 + tx;
+        if (ix >= pr.K[0]) ix -= pr.K[0];
+        float p = 0.f, py = 0.f;  // sum over y of P wy, P dy
+#pragma unroll
+        for (int ty = 0; ty < ORDER; ty++) {
+          int iy = iy0 + ty;
+          if (iy >= pr.K[1]) iy -= pr.K[1];
+          const float P = __ldg(base + ((size_t)ix * pr.K[1] + iy) * pr.K[2] + iz);
+          p = fmaf(P, wy[ty], p);
+          py = fmaf(P, dy[ty], py);
+        }
+        phi = fmaf(wx[tx], p, phi);
+        gx = fmaf(dx[tx], p, gx);
+        gy = fmaf(wx[tx], py, gy);
+      }
+      gz = phi * dzg;
+      phi *= wzg;
+      gx *= wzg;
+      gy *= wzg;
+    }
+  }
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) {
+    phi += __shfl_xor_sync(kFull, phi, o);
+    gx += __shfl_xor_sync(kFull, gx, o);
+    gy += __shfl_xor_sync(kFull, gy, o);
+    gz += __shfl_xor_sync(kFull, gz, o);
+  }
+  float e = 0.f;
+  if (valid && g == 0) {
+    const RepInfo &ri = a.rep[r];
+    const float c = 2.f * qe;
+    const float fx = c * gx * ((float)pr.K[0] / ri.box[0]);
+    const float fy = c * gy * ((float)pr.K[1] / ri.box[1]);
+    const float fz = c * gz * ((float)pr.K[2] / ri.box[2]);
+    if (o.force64) {
+      o.force64[3 * atom] = fx;
+      o.force64[3 * atom + 1] = fy;
+      o.force64[3 * atom + 2] = fz;
+    }
+    if (o.force) {
+      atomicAdd(&o.force[3 * atom], fx);
+      atomicAdd(&o.force[3 * atom + 1], fy);
+      atomicAdd(&o.force[3 * atom + 2], fz);
+    }
+    if (block) red_add(&a.accL[block], to_fix(2.f * qraw * phi));
+    if (ENERGY) e = qe * phi;
+  }
+  if (ENERGY) {
+    // one atomic per warp when its 4 atoms share a replica
+    const int r0 = __shfl_sync(kFull, r, 0);
+    const bool same = __all_sync(kFull, !valid || r == r0);
+    long long ef = to_fix(e);
+    if (same) {
+#pragma unroll
+      for (int o2 = 16; o2 > 0; o2 >>= 1) ef += __shfl_xor_sync(kFull, ef, o2);
+      if (lane == 0 && ef) red_add(&a.accE[r0], ef);
+    } else if (ef) {
+      red_add(&a.accE[r], ef);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Ewald self term: one thread per atom.
+// ---------------------------------------------------------------------------
+template <bool ENERGY>
+__global__ void k_self(PmeArgs a, float pre) {
+  const int lane = threadIdx.x & 31;
+  const int atom = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = atom < a.N;
+  float e = 0.f;
+  int r = 0;
+  if (valid) {
+    r = a.atomRep[atom];
+    int block;
+    const float l = atom_scale(a, atom, block);
+    const float q = a.q[atom];
+    const float es = pre * q * q;
+    if (block) red_add(&a.accL[block], to_fix(2.f * l * es));
+    e = l * l * es;
+  }
+  if (ENERGY) {
+    const int r0 = __shfl_sync(kFull, r, 0);
+    const bool same = __all_sync(kFull, !valid || r == r0);
+    long long ef = to_fix(e);
+    if (same) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) ef += __shfl_xor_sync(kFull, ef, o);
+      if (lane == 0 && ef) red_add(&a.accE[r0], ef);
+    } else if (ef) {
+      red_add(&a.accE[r], ef);
+    }
+  }
+}
+
+// lambda and energy accumulators -> outputs (one CTA).
+__global__ void k_pme_finalize(PmeArgs a, bnb_outputs o, bool energy) {
+  const double inv = 1.0 / kFixScale;
+  for (int i = threadIdx.x; i < a.lamTotal; i += blockDim.x) {
+    const long long v = a.accL[i];
+    a.accL[i] = 0;
+    const double f = (double)v * inv;
+    if (o.lambdaForce64) o.lambdaForce64[i] = f;
+    if (o.lambdaForce && v) atomicAdd(&o.lambdaForce[i], (float)f);
+  }
+  if (energy)
+    for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
+      const long long v = a.accE[r];
+      a.accE[r] = 0;
+      const double e = (double)v * inv;
+      if (o.energy64) o.energy64[r] = e;
+      if (o.energy) o.energy[r] += e;
+    }
+}
+
+inline int grid_of(long long threads, int block) {
+  long long g = (threads + block - 1) / block;
+  return (int)(g < 1 ? 1 : (g > 148LL * 64 ? 148LL * 64 : g));
+}
+
+}  // namespace
+
+int pme_spread(const PmeArgs &a, cudaStream_t s) {
+  if (a.N > 0) {
+    const int grid = (int)((8LL * a.N + 255) / 256);
+    switch (a.order) {
+      case 4: k_spread<4><<<grid, 256, 0, s>>>(a); break;
+      case 6: k_spread<6><<<grid, 256, 0, s>>>(a); break;
+      case 8: k_spread<8><<<grid, 256, 0, s>>>(a); break;
+      default: return BNB_ERR_ARG;
+    }
+  }
+  k_fix_to_grid<<<grid_of(a.totalGrid, 256), 256, 0, s>>>(a);
+  return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
+}
+
+int pme_convolve(const PmeArgs &a, cudaStream_t s) {
+  int gx = (a.maxCplx + 1023) / 1024;  // about 4 elements per thread
+  gx = gx < 1 ? 1 : gx;
+  k_convolve<<<dim3(gx, a.R), 256, 0, s>>>(a);
+  return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
+}
+
+int pme_gather(const PmeArgs &a, const bnb_outputs &o, bool energy, cudaStream_t s) {
+  if (a.N > 0) {
+    const int grid = (int)((8LL * a.N + 255) / 256);
+    switch (a.order * 2 + (energy ? 1 : 0)) {
+      case 8: k_gather<4, false><<<grid, 256, 0, s>>>(a, o); break;
+      case 9: k_gather<4, true><<<grid, 256, 0, s>>>(a, o); break;
+      case 12: k_gather<6, false><<<grid, 256, 0, s>>>(a, o); break;
+      case 13: k_gather<6, true><<<grid, 256, 0, s>>>(a, o); break;
+      case 16: k_gather<8, false><<<grid, 256, 0, s>>>(a, o); break;
+      case 17: k_gather<8, true><<<grid, 256, 0, s>>>(a, o); break;
+      default: return BNB_ERR_ARG;
+    }
+  }
+  k_pme_finalize<<<1, 256, 0, s>>>(a, o, energy);
+  return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
+}
+
+int pme_self(const PmeArgs &a, const bnb_outputs &o, bool energy, cudaStream_t s) {
+  // -beta / sqrt(pi) (kElectric is inside the scaled charges)
+  const float pre = (float)(-(double)a.beta / sqrt(kPi));
+  if (a.N > 0) {
+    const int grid = (a.N + 255) / 256;
+    if (energy) k_self<true><<<grid, 256, 0, s>>>(a, pre);
+    else k_self<false><<<grid, 256, 0, s>>>(a, pre);
+  }
+  k_pme_finalize<<<1, 256, 0, s>>>(a, o, energy);
+  return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
+}
+
+}  // namespace bnb

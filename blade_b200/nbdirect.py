@@ -157,6 +157,57 @@ class NbDirect:
         self.getforce_pairs(which, pos, lam, calc_energy, force64=f64, lambda_force64=l64, energy64=e64)
         return f64.reshape(-1, 3), l64, e64
 
+    # -- PME reciprocal space and Ewald self term (getforce_ewald / getforce_ewaldself)
+    def set_pme(self, order: int = 6, grid_space: float = 1.0, grid=None):
+        """bnb_set_pme: one grid per replica, from ``grid`` ([R,3] sizes) or
+        the reference's rule for ``grid_space`` (Run::gridSpace, 1 A)."""
+        b = np.ascontiguousarray(self.boxes, np.float32)
+        g = None if grid is None else np.ascontiguousarray(np.broadcast_to(np.asarray(grid, np.int32),
+                                                                           (self.R, 3)))
+        _lib.call("bnb_set_pme", self.h, int(order), float(grid_space),
+                  None if g is None else g.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p))
+
+    def pme_grid(self, replica: int = 0):
+        K = np.zeros(3, np.int32)
+        _lib.call("bnb_pme_grid", self.h, int(replica), K.ctypes.data_as(C.c_void_p))
+        return tuple(int(k) for k in K)
+
+    def getforce_ewald(self, positions, lambdas=None, calc_energy=True, force=None, lambda_force=None,
+                       energy=None, force64=None, lambda_force64=None, energy64=None, stream=None, boxes=None):
+        """bnb_compute_pme (getforce_ewald)."""
+        out = _lib.Outputs(force=_ptr(force), lambdaForce=_ptr(lambda_force), energy=_ptr(energy),
+                           force64=_ptr(force64), lambdaForce64=_ptr(lambda_force64), energy64=_ptr(energy64))
+        b = np.ascontiguousarray(self.boxes if boxes is None else boxes, np.float32)
+        _lib.call("bnb_compute_pme", self.h, _ptr(positions), _ptr(lambdas), b.ctypes.data_as(C.c_void_p),
+                  int(bool(calc_energy)), C.byref(out), _stream(stream))
+
+    def getforce_ewaldself(self, lambdas=None, calc_energy=True, lambda_force=None, energy=None,
+                           lambda_force64=None, energy64=None, stream=None):
+        """bnb_compute_ewald_self (getforce_ewaldself)."""
+        out = _lib.Outputs(lambdaForce=_ptr(lambda_force), energy=_ptr(energy), lambdaForce64=_ptr(lambda_force64),
+                           energy64=_ptr(energy64))
+        _lib.call("bnb_compute_ewald_self", self.h, _ptr(lambdas), int(bool(calc_energy)), C.byref(out),
+                  _stream(stream))
+
+    def evaluate_pme(self, positions=None, lambdas=None, calc_energy=True):
+        """Reciprocal term with fresh FP64 outputs: (dU/dx [N,3], dU/dlambda [L], energy [R])."""
+        import torch
+        pos = self.positions_tensor() if positions is None else positions
+        lam = self.lambdas_tensor() if lambdas is None else lambdas
+        f64 = torch.zeros(3 * self.N, dtype=torch.float64, device=self.device)
+        l64 = torch.zeros(self.L, dtype=torch.float64, device=self.device)
+        e64 = torch.zeros(self.R, dtype=torch.float64, device=self.device)
+        self.getforce_ewald(pos, lam, calc_energy, force64=f64, lambda_force64=l64, energy64=e64)
+        return f64.reshape(-1, 3), l64, e64
+
+    def evaluate_ewald_self(self, lambdas=None):
+        import torch
+        lam = self.lambdas_tensor() if lambdas is None else lambdas
+        l64 = torch.zeros(self.L, dtype=torch.float64, device=self.device)
+        e64 = torch.zeros(self.R, dtype=torch.float64, device=self.device)
+        self.getforce_ewaldself(lam, True, lambda_force64=l64, energy64=e64)
+        return l64, e64
+
     # -- conveniences ------------------------------------------------------------
     def positions_tensor(self, xyz_list=None):
         import torch

@@ -108,6 +108,86 @@ def run_msld(args, water_only=False):
     print(json.dumps(line), flush=True)
 
 
+def run_pme(args):
+    """PME reciprocal space: device time per evaluation of bnb_compute_pme and
+    of the reference's getforce_ewald (its CUDA build, same GPU) on the
+    23,558-atom chain-in-water system (64^3 grid, order 6) and the water box
+    (20^3), error against the FP64 oracle, and the 64 batch replicas on one
+    handle against one handle per replica."""
+    import torch
+    from oracle import pme_oracle, refgpu
+    from .nbdirect import NbDirect
+    K_E = 332.0716
+    out = {"config": "PME reciprocal space, order 6, grids from 1 A spacing; energy every 10th evaluation"}
+    reps = args.steps
+
+    def time_calls(fn, n):
+        for k in range(10):
+            fn(k)
+        a, b = _events()
+        a.record()
+        for k in range(n):
+            fn(k)
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / n
+
+    parts = set(args.parts.split(","))
+    singles_sys = (("chain_water_23558", systems.chain_in_water()), ("water216", systems.water_box()))
+    for name, s in (singles_sys if "single" in parts else ()):
+        nb = NbDirect(s)
+        nb.set_pme(order=6, grid_space=1.0)
+        K = nb.pme_grid(0)
+        pos = nb.positions_tensor()
+        f64, _, e64 = nb.evaluate_pme(pos)
+        E, g, _, _ = pme_oracle.pme_recip(s.xyz, s.nbonds["q"], s.box, K, 6, s.betaEwald, K_E)
+        force = torch.zeros(3 * s.N, device="cuda")
+        energy = torch.zeros(1, dtype=torch.float64, device="cuda")
+        ms = time_calls(lambda k: nb.getforce_ewald(pos, None, k % 10 == 0, force=force, energy=energy), reps)
+        line = {"atoms": s.N, "grid": K, "bnb_ms_per_eval": ms,
+                "force_rel_rms_vs_fp64": float(np.sqrt(((f64.cpu().numpy() - g) ** 2).sum() / (g ** 2).sum())),
+                "energy_rel_err_vs_fp64": abs(float(e64.cpu()[0]) - E) / abs(E)}
+        if refgpu.available():
+            ref = refgpu.RefGPU(s)
+            ref.set_pme(6, K)
+            r = ref.evaluate_pme("recip")
+            ref.time_pme(10)
+            line["reference_ms_per_eval"] = ref.time_pme(reps) / reps
+            line["reference_force_rel_rms_vs_fp64"] = float(np.sqrt(((r["grad"] - g) ** 2).sum() / (g ** 2).sum()))
+        out[name] = line
+        nb.close()
+    if "batch" not in parts:
+        print(json.dumps(out), flush=True)
+        return
+    # batch: 64 replicas of 3k-30k atoms, one handle vs one handle per replica
+    reps_sys = systems.batch_replicas(args.replicas, seed=args.seed)
+    nb = NbDirect(reps_sys)
+    nb.set_pme(order=6, grid_space=1.0)
+    pos = nb.positions_tensor()
+    lam = nb.lambdas_tensor()
+    force = torch.zeros(3 * nb.N, device="cuda")
+    lforce = torch.zeros(nb.L, device="cuda")
+    ms_b = time_calls(lambda k: nb.getforce_ewald(pos, lam, False, force=force, lambda_force=lforce), 50)
+    singles = []
+    for s in reps_sys:
+        one = NbDirect(s)
+        one.set_pme(order=6, grid_space=1.0)
+        singles.append((one, one.positions_tensor(), one.lambdas_tensor(),
+                        torch.zeros(3 * s.N, device="cuda"), torch.zeros(one.L, device="cuda")))
+
+    def all_singles(k):
+        for one, p, l, f, lf in singles:
+            one.getforce_ewald(p, l, False, force=f, lambda_force=lf)
+    ms_s = time_calls(all_singles, 20)
+    out["batch"] = {"replicas": len(reps_sys), "atoms": nb.N, "batched_ms_per_eval": ms_b,
+                    "one_handle_per_replica_ms_per_eval": ms_s, "speedup": ms_s / ms_b,
+                    "distinct_grids": len({tuple(nb.pme_grid(r)) for r in range(nb.R)})}
+    for one, *_ in singles:
+        one.close()
+    nb.close()
+    print(json.dumps(out), flush=True)
+
+
 def run_batch(args):
     import torch
     from .batch import MsldBatch, ns_per_day
@@ -313,7 +393,7 @@ def run_alf(args):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["water", "msld", "batch", "alf"])
+    ap.add_argument("what", choices=["water", "msld", "batch", "alf", "pme"])
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--seed", type=int, default=4)
@@ -328,11 +408,14 @@ def main(argv=None):
     ap.add_argument("--model-in", default=None)
     ap.add_argument("--eval-modes", default="plain,learned:1")
     ap.add_argument("--target", default="flat", choices=["flat", "lookahead"])
+    ap.add_argument("--parts", default="single,batch", help="pme: single (one system) and/or batch")
     args, rest = ap.parse_known_args(argv)
     if args.what in ("msld", "water"):
         run_msld(args, water_only=args.what == "water")
     elif args.what == "batch":
         run_batch(args)
+    elif args.what == "pme":
+        run_pme(args)
     else:
         run_alf(args)
 

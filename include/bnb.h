@@ -213,6 +213,34 @@ int bnb_compute_nbex(bnb_handle *h, const float *position, const float *lambda,
                      const float *boxes, int calcEnergy, const bnb_outputs *out, void *stream);
 
 /*
+ * PME reciprocal space and the Ewald self term (getforce_ewald and
+ * getforce_ewaldself, src/nbrecip/nbrecip.cu:19-555; grids and B-spline
+ * moduli as Potential::initialize, src/system/potential.cxx:1202-1300).
+ * bnb_set_pme sizes one grid per replica and makes the cuFFT plans:
+ *   order    B-spline order 4, 6 or 8 (Run::orderEwald, default 6)
+ *   gridSpace, grid  host int [3*replicas] grid sizes, or NULL for the
+ *            reference's rule from the spacing (Run::gridSpace, default 1 A):
+ *            per edge the smallest of j*{32,27,24,20,18} above L/gridSpace
+ *   boxes    host float [3*replicas] edges the grids are sized for
+ * Charges, MSLD blocks and replicas come from bnb_set_topology; an atom of
+ * block b > 0 carries lambda_b q (Msld atomBlock, nbrecip.cu:101-106).
+ * bnb_compute_pme evaluates the reciprocal term (spread, R2C, influence
+ * function, C2R, gather) on position (device float [3N], State::position_fd)
+ * and lambda (device float, State::lambda_fd) with the box edges `boxes`
+ * (host float [3*replicas]; the grids stay as set), into `out` with
+ * bnb_compute's output semantics; energies are the eenbrecip term.
+ * bnb_compute_ewald_self adds the self term (energy eenbrecipself and
+ * dU/dlambda; no spatial force).  Both do nothing unless elecMethod is PME
+ * (as the reference).  bnb_pme_grid returns the grid of one replica.
+ */
+int bnb_set_pme(bnb_handle *h, int order, float gridSpace, const int *grid, const float *boxes);
+int bnb_pme_grid(bnb_handle *h, int replica, int *K);
+int bnb_compute_pme(bnb_handle *h, const float *position, const float *lambda,
+                    const float *boxes, int calcEnergy, const bnb_outputs *out, void *stream);
+int bnb_compute_ewald_self(bnb_handle *h, const float *lambda, int calcEnergy,
+                           const bnb_outputs *out, void *stream);
+
+/*
  * Sets list capacities (candidate tiles, 32-row exclusion masks, work items)
  * before the next rebuild; values <= 0 keep the current/estimated size.  The
  * counterpart of the reference's maxPartnersPerBlock / maxBlockExclCount

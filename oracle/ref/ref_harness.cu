@@ -13,8 +13,11 @@
 // Each step it calls Domdec::update_domdec and getforce_nbdirect exactly as
 // Run::dynamics and Potential::calc_force do (src/run/run.cu:554-564,
 // src/system/potential.cxx:1839-1929), on one stream; ref_evaluate_pairs
-// calls getforce_nb14 / getforce_nbex (src/bonded/pair.cu) the same way.
+// calls getforce_nb14 / getforce_nbex (src/bonded/pair.cu) the same way, and
+// ref_evaluate_pme getforce_ewald / getforce_ewaldself (src/nbrecip/nbrecip.cu)
+// on PME grids set up as Potential::initialize does (potential.cxx:1202-1300).
 #include <cuda_runtime.h>
+#include <cufft.h>
 
 #include <cmath>
 #include <cstdarg>
@@ -29,6 +32,7 @@
 #include "main/defines.h"
 #include "msld/msld.h"
 #include "nbdirect/nbdirect.h"
+#include "nbrecip/nbrecip.h"
 #include "run/run.h"
 #include "system/potential.h"
 #include "system/state.h"
@@ -316,3 +320,122 @@ extern "C" int ref_evaluate_pairs(ref_handle *h, int which, int calcEnergy, doub
   return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
+
+// PME grids, B-spline moduli, cuFFT plans and per-atom charges/blocks as
+// Potential::initialize / Msld set them up (potential.cxx:1202-1300), for the
+// grid K[3] and interpolation order given.  q: raw charges [N]; block: the
+// atom's lambda block (0 = environment) [N].
+extern "C" int ref_set_pme(ref_handle *h, int order, const int *K, const float *q, const int *block) {
+  System *sys = h->sys;
+  Potential *pot = h->pot;
+  Run *run = h->run;
+  State *st = h->st;
+  const int N = h->N;
+  run->orderEwald = order;
+  run->calcTermFlag[eenbrecip] = true;
+  run->calcTermFlag[eenbrecipself] = true;
+  st->kOrthBox_f.x = 1 / st->orthBox_f.x;
+  st->kOrthBox_f.y = 1 / st->orthBox_f.y;
+  st->kOrthBox_f.z = 1 / st->orthBox_f.z;
+  for (int k = 0; k < 3; k++) pot->gridDimPME[k] = K[k];
+  const size_t nr = (size_t)K[0] * K[1] * K[2], nc = (size_t)K[0] * K[1] * (K[2] / 2 + 1);
+  cudaMalloc(&pot->charge_d, sizeof(float) * (N > 0 ? N : 1));
+  cudaMemcpy(pot->charge_d, q, sizeof(float) * N, cudaMemcpyHostToDevice);
+  cudaMalloc(&sys->msld->atomBlock_d, sizeof(int) * (N > 0 ? N : 1));
+  cudaMemcpy(sys->msld->atomBlock_d, block, sizeof(int) * N, cudaMemcpyHostToDevice);
+  cudaMalloc(&pot->chargeGridPME_d, sizeof(cufftReal) * nr);
+  cudaMalloc(&pot->fourierGridPME_d, sizeof(cufftComplex) * nc);
+  cudaMalloc(&pot->potentialGridPME_d, sizeof(cufftReal) * nr);
+  {
+    cudaResourceDesc rd;
+    memset(&rd, 0, sizeof(rd));
+    rd.resType = cudaResourceTypeLinear;
+    rd.res.linear.devPtr = pot->potentialGridPME_d;
+    rd.res.linear.desc = cudaCreateChannelDesc<float>();
+    rd.res.linear.sizeInBytes = sizeof(float) * nr;
+    cudaTextureDesc td;
+    memset(&td, 0, sizeof(td));
+    td.readMode = cudaReadModeElementType;
+    if (cudaCreateTextureObject(&pot->potentialGridPME_tex, &rd, &td, NULL) != cudaSuccess) return 2;
+  }
+  // 1/|b(m)|^2 per dimension from M_n at the integers, product over the half grid
+  double M[12] = {0};
+  M[1] = 1.0;
+  for (int k = 3; k <= order; k++) {
+    double nw[12] = {0};
+    for (int l = 0; l <= k; l++) nw[l] = (l * M[l] + (k - l) * (l >= 1 ? M[l - 1] : 0.0)) / (k - 1);
+    for (int l = 0; l < 12; l++) M[l] = nw[l];
+  }
+  float *inv[3];
+  for (int d = 0; d < 3; d++) {
+    inv[d] = (float *)malloc(sizeof(float) * K[d]);
+    for (int m = 0; m < K[d]; m++) {
+      double re = 0, im = 0;
+      for (int l = 1; l < order; l++) {
+        re += M[l] * cos(2 * M_PI * m * l / K[d]);
+        im += M[l] * sin(2 * M_PI * m * l / K[d]);
+      }
+      inv[d][m] = (float)(1.0 / (re * re + im * im));
+    }
+  }
+  float *bg = (float *)malloc(sizeof(float) * nc);
+  for (int i = 0; i < K[0]; i++)
+    for (int j = 0; j < K[1]; j++)
+      for (int k = 0; k < K[2] / 2 + 1; k++)
+        bg[((size_t)i * K[1] + j) * (K[2] / 2 + 1) + k] = inv[0][i] * inv[1][j] * inv[2][k];
+  cudaMalloc(&pot->bGridPME_d, sizeof(float) * nc);
+  cudaMemcpy(pot->bGridPME_d, bg, sizeof(float) * nc, cudaMemcpyHostToDevice);
+  free(bg);
+  for (int d = 0; d < 3; d++) free(inv[d]);
+  if (cufftPlan3d(&pot->planFFTPME, K[0], K[1], K[2], CUFFT_R2C) != CUFFT_SUCCESS) return 2;
+  if (cufftPlan3d(&pot->planIFFTPME, K[0], K[1], K[2], CUFFT_C2R) != CUFFT_SUCCESS) return 2;
+  cufftSetStream(pot->planFFTPME, h->stream);
+  cufftSetStream(pot->planIFFTPME, h->stream);
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// One reciprocal (which 0) or self (which 1) evaluation on the current state.
+extern "C" int ref_evaluate_pme(ref_handle *h, int which, int calcEnergy, double *grad, double *energy,
+                                double *lambdaForce) {
+  System *sys = h->sys;
+  State *st = h->st;
+  st->broadcast_position(sys);
+  cudaMemsetAsync(st->forceBuffer_d, 0, sizeof(float) * (3 * h->N + 2 * h->nL), h->stream);
+  cudaMemsetAsync(st->energy_d, 0, sizeof(double) * eeend, h->stream);
+  if (which == 0) getforce_ewald(sys, calcEnergy != 0);
+  else getforce_ewaldself(sys, calcEnergy != 0);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return 2;
+  int n = 3 * h->N;
+  float *tmp = (float *)malloc(sizeof(float) * (n + h->nL));
+  cudaMemcpy(tmp, st->force_d, sizeof(float) * n, cudaMemcpyDeviceToHost);
+  for (int i = 0; i < n; i++) grad[i] = tmp[i];
+  if (lambdaForce) {
+    cudaMemcpy(tmp, st->lambdaForce_d, sizeof(float) * h->nL, cudaMemcpyDeviceToHost);
+    for (int i = 0; i < h->nL; i++) lambdaForce[i] = tmp[i];
+  }
+  free(tmp);
+  if (energy)
+    cudaMemcpy(energy, st->energy_d + (which == 0 ? eenbrecip : eenbrecipself), sizeof(double),
+               cudaMemcpyDeviceToHost);
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// Device time of `reps` reciprocal evaluations (getforce_ewald alone, energy
+// every `energyEvery`-th call), summed over CUDA events on the path's stream.
+extern "C" int ref_time_pme(ref_handle *h, int reps, int energyEvery, double *ms) {
+  System *sys = h->sys;
+  State *st = h->st;
+  st->broadcast_position(sys);
+  double total = 0;
+  for (int k = 0; k < reps; k++) {
+    cudaEventRecord(h->e0, h->stream);
+    getforce_ewald(sys, energyEvery > 0 && k % energyEvery == 0);
+    cudaEventRecord(h->e1, h->stream);
+    cudaEventSynchronize(h->e1);
+    float t = 0;
+    cudaEventElapsedTime(&t, h->e0, h->e1);
+    total += t;
+  }
+  *ms = total;
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}

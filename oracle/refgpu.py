@@ -30,6 +30,9 @@ def lib():
         L.ref_list_info.argtypes = [p, p, p]
         L.ref_set_pairs.argtypes = [p, i, p, i, p, i]
         L.ref_evaluate_pairs.argtypes = [p, i, i, p, p, p]
+        L.ref_set_pme.argtypes = [p, i, p, p, p]
+        L.ref_evaluate_pme.argtypes = [p, i, i, p, p, p]
+        L.ref_time_pme.argtypes = [p, i, i, p]
         _lib = L
     return _lib
 
@@ -96,6 +99,34 @@ class RefGPU:
         if rc != 0:
             raise RuntimeError("reference harness: evaluate_pairs failed")
         return {"grad": g.reshape(-1, 3), "energy": float(e[0]), "lambdaForce": lf}
+
+    def set_pme(self, order, K):
+        """PME grids and plans for grid K (3 sizes) and B-spline order."""
+        self._K = np.ascontiguousarray(K, np.int32)
+        self._q = np.ascontiguousarray(self.sys.nbonds["q"], np.float32)
+        self._blk = np.ascontiguousarray(self.sys.nbonds["siteBlock"] & 0xFFFF, np.int32)
+        P = lambda a: a.ctypes.data_as(C.c_void_p)
+        if lib().ref_set_pme(self.h, int(order), P(self._K), P(self._q), P(self._blk)) != 0:
+            raise RuntimeError("reference harness: set_pme failed")
+
+    def evaluate_pme(self, which="recip", xyz=None, lam=None, energy=True):
+        """getforce_ewald (which="recip") or getforce_ewaldself (which="self") of the reference."""
+        self.set_state(self.sys.xyz if xyz is None else xyz, self.sys.lambdas() if lam is None else lam)
+        g = np.zeros(3 * self.N)
+        e = np.zeros(1)
+        lf = np.zeros(self.nL)
+        rc = lib().ref_evaluate_pme(self.h, 0 if which == "recip" else 1, int(energy), g.ctypes.data_as(C.c_void_p),
+                                    e.ctypes.data_as(C.c_void_p), lf.ctypes.data_as(C.c_void_p))
+        if rc != 0:
+            raise RuntimeError("reference harness: evaluate_pme failed")
+        return {"grad": g.reshape(-1, 3), "energy": float(e[0]), "lambdaForce": lf}
+
+    def time_pme(self, reps, energy_every=10):
+        """Device time (ms) of `reps` getforce_ewald calls on the current state."""
+        ms = C.c_double()
+        if lib().ref_time_pme(self.h, int(reps), int(energy_every), C.byref(ms)) != 0:
+            raise RuntimeError("reference harness: time_pme failed")
+        return ms.value
 
     def time(self, frames_d, steps, rebuild_every=10, energy_every=10, flush=None):
         """Device time (ms) of `steps` steps over a torch float64 CUDA tensor [steps, 3N]."""

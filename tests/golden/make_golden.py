@@ -12,7 +12,11 @@ the MSLD water box (soft core on and off), and the 23,558-atom chain-in-water
 system (forces of the first 3,000 atoms kept); and, from the reference's
 getforce_nb14 / getforce_nbex (src/bonded/pair.cu), pairs_*.npz for a small
 chain-in-water system (1-4 pairs with e14fac 0.5 under three method
-combinations, PME exclusion corrections) and the MSLD water box.
+combinations, PME exclusion corrections) and the MSLD water box; and, from
+the reference's getforce_ewald / getforce_ewaldself (src/nbrecip/nbrecip.cu),
+pme_*.npz: reciprocal-space dU/dx, energy and dU/dlambda plus the self term
+for the water box (orders 4, 6, 8), the MSLD water box and a small
+chain-in-water system (--pme-only makes just these).
 """
 import os
 import sys
@@ -54,8 +58,33 @@ def pair_cases():
     yield "pairs_msld_nbex", m, "nbex", False, None
 
 
-def main(out, pairs_only=False):
+def pme_cases():
+    """(name, system, order, grid) of the PME fixtures; grids from 1 A spacing."""
+    from oracle import pme_oracle
+    for order in (4, 6, 8):
+        s = systems.water_box()
+        yield f"pme_water216_o{order}", s, order, [pme_oracle.grid_size(L, 1.0) for L in s.box]
+    s = systems.msld_water()
+    yield "pme_msld_water", s, 6, [pme_oracle.grid_size(L, 1.0) for L in s.box]
+    s = systems.chain_in_water(seed=5, box=30.0, n_chain=250, n_wat=780, name="chain_water_small")
+    yield "pme_chain_small", s, 6, [pme_oracle.grid_size(L, 1.0) for L in s.box]
+
+
+def main(out, pairs_only=False, pme_only=False):
     os.makedirs(out, exist_ok=True)
+    for name, s, order, K in pme_cases():
+        ref = refgpu.RefGPU(s)
+        ref.set_pme(order, K)
+        r = ref.evaluate_pme("recip")
+        r2 = ref.evaluate_pme("self")
+        np.savez_compressed(os.path.join(out, name + ".npz"), xyz=s.xyz.astype(np.float32),
+                            grad=r["grad"].astype(np.float32), energy=np.float64(r["energy"]),
+                            lambdaForce=r["lambdaForce"].astype(np.float64),
+                            self_energy=np.float64(r2["energy"]), self_lambdaForce=r2["lambdaForce"].astype(np.float64),
+                            K=np.int64(K), order=np.int64(order), beta=np.float64(s.betaEwald))
+        print(name, K, order, r["energy"], r2["energy"], flush=True)
+    if pme_only:
+        return
     for name, s, keep in ([] if pairs_only else cases()):
         r = refgpu.RefGPU(s).evaluate()
         g = r["grad"].astype(np.float32)
@@ -79,4 +108,5 @@ def main(out, pairs_only=False):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    main(args[0] if args else os.path.join(ROOT, "golden_out"), pairs_only="--pairs-only" in sys.argv)
+    main(args[0] if args else os.path.join(ROOT, "golden_out"), pairs_only="--pairs-only" in sys.argv,
+         pme_only="--pme-only" in sys.argv)

@@ -1,0 +1,93 @@
+"""The FP64 PME restatement (oracle/pme_oracle.py) on its own: the grid rule
+of Potential::initialize, B-spline identities, convergence to the plain Ewald
+reciprocal sum, and finite-difference checks of dU/dx and dU/dlambda."""
+import numpy as np
+import pytest
+
+from blade_b200 import systems
+from oracle import pme_oracle as P
+
+K_ELECTRIC = 332.0716
+
+
+def test_grid_rule():
+    # L / spacing -> smallest of j*{32,27,24,20,18} above it (potential.cxx:1204-1218)
+    cases = {62.23: 64, 18.856: 20, 40.0: 48, 100.0: 108, 12.0: 18, 30.0: 32, 25.14: 27, 17.9: 18, 33.0: 36}
+    for L, K in cases.items():
+        assert P.grid_size(L, 1.0) == K, L
+    assert P.grid_size(62.23, 0.5) == 128
+
+
+def test_bspline_identities():
+    f = np.linspace(0.0, 0.999, 17)
+    for n in (4, 6, 8):
+        w, d = P.weights(f, n)
+        assert np.allclose(w.sum(-1), 1.0, atol=1e-14)      # partition of unity
+        assert np.allclose(d.sum(-1), 0.0, atol=1e-14)
+        assert np.all(w >= 0)
+        M = P.bspline_int(n)
+        assert M.sum() == pytest.approx(1.0)
+        # weights at f = 0 are M_n at the integers n-1 .. 0
+        w0, _ = P.weights(np.zeros(1), n)
+        assert np.allclose(w0[0], M[n - 1::-1][:n])
+        h = 1e-6
+        fi = f[1:]                                           # interior points: f - h stays >= 0
+        wp, _ = P.weights(fi + h, n)
+        wm, _ = P.weights(fi - h, n)
+        assert np.allclose((wp - wm) / (2 * h), d[1:], atol=1e-6)
+
+
+def test_converges_to_ewald_sum():
+    s = systems.water_box()
+    q = s.nbonds["q"].astype(np.float64)
+    E0, g0 = P.ewald_recip_exact(s.xyz, q, s.box, 0.34, K_ELECTRIC, kmax=12)
+    E, g, _, _ = P.pme_recip(s.xyz, q, s.box, [48, 48, 48], 8, 0.34, K_ELECTRIC)
+    assert E == pytest.approx(E0, rel=1e-8)
+    assert np.sqrt(((g - g0) ** 2).sum() / (g0 ** 2).sum()) < 1e-8
+    # the reference's default (1 A grid, order 6) is within 1e-4
+    E6, g6, _, _ = P.pme_recip(s.xyz, q, s.box, [20, 20, 20], 6, 0.34, K_ELECTRIC)
+    assert E6 == pytest.approx(E0, rel=2e-4)
+
+
+def test_finite_differences():
+    s = systems.msld_water()
+    q = s.nbonds["q"].astype(np.float64)
+    sb = s.nbonds["siteBlock"]
+    lam = s.lambdas().astype(np.float64)
+    K = [P.grid_size(L, 1.0) for L in s.box]
+    E, g, lf, _ = P.pme_recip(s.xyz, q, s.box, K, 6, s.betaEwald, K_ELECTRIC, sb, lam)
+    x0 = s.xyz.astype(np.float64)
+    h = 1e-5
+    pert = np.nonzero(sb & 0xFFFF)[0]
+    for i in (0, 7, int(pert[0]), int(pert[-1])):
+        for d in range(3):
+            xp = x0.copy(); xp[i, d] += h
+            xm = x0.copy(); xm[i, d] -= h
+            fd = (P.pme_recip(xp, q, s.box, K, 6, s.betaEwald, K_ELECTRIC, sb, lam)[0]
+                  - P.pme_recip(xm, q, s.box, K, 6, s.betaEwald, K_ELECTRIC, sb, lam)[0]) / (2 * h)
+            assert fd == pytest.approx(g[i, d], rel=1e-5, abs=1e-6)
+    for b in range(1, len(lam)):
+        lp = lam.copy(); lp[b] += 1e-6
+        lm = lam.copy(); lm[b] -= 1e-6
+        fd = (P.pme_recip(x0, q, s.box, K, 6, s.betaEwald, K_ELECTRIC, sb, lp)[0]
+              - P.pme_recip(x0, q, s.box, K, 6, s.betaEwald, K_ELECTRIC, sb, lm)[0]) / 2e-6
+        assert fd == pytest.approx(lf[b], rel=1e-5, abs=1e-5)
+    Es, ls = P.ewald_self(q, s.betaEwald, K_ELECTRIC, sb, lam)
+    for b in range(1, len(lam)):
+        lp = lam.copy(); lp[b] += 1e-6
+        lm = lam.copy(); lm[b] -= 1e-6
+        fd = (P.ewald_self(q, s.betaEwald, K_ELECTRIC, sb, lp)[0] - P.ewald_self(q, s.betaEwald, K_ELECTRIC, sb, lm)[0]) / 2e-6
+        assert fd == pytest.approx(ls[b], rel=1e-6, abs=1e-6)
+
+
+def test_translation_invariance():
+    """A shift of every atom by whole grid cells leaves energy and forces
+    unchanged (the grid convention is a translation of the reference's)."""
+    s = systems.water_box()
+    q = s.nbonds["q"].astype(np.float64)
+    K = [20, 20, 20]
+    E, g, _, _ = P.pme_recip(s.xyz, q, s.box, K, 6, 0.34, K_ELECTRIC)
+    shift = np.float64(s.box[0]) / 20 * np.array([3, -1, 7])
+    E2, g2, _, _ = P.pme_recip(s.xyz.astype(np.float64) + shift, q, s.box, K, 6, 0.34, K_ELECTRIC)
+    assert E2 == pytest.approx(E, rel=1e-10)
+    assert np.allclose(g2, g, atol=1e-8)
