@@ -36,6 +36,11 @@ class Outputs(C.Structure):
                 ("force64", C.c_void_p), ("lambdaForce64", C.c_void_p), ("energy64", C.c_void_p)]
 
 
+class ConstraintSet(C.Structure):
+    _fields_ = [("nTriangle", C.c_int), ("nBranch1", C.c_int), ("nBranch2", C.c_int), ("nBranch3", C.c_int),
+                ("triangle", C.c_void_p), ("branch1", C.c_void_p), ("branch2", C.c_void_p), ("branch3", C.c_void_p)]
+
+
 _lib = None
 
 
@@ -75,6 +80,10 @@ def lib():
             "bnb_compute_nb14": (i, [p, p, p, p, i, p, p]),
             "bnb_compute_nbex": (i, [p, p, p, p, i, p, p]),
             "bnb_nbdirect_noalloc": (i, [p, i, p, p, p, i, p, p, p, i, p, p]),
+            "bnb_holonomic_position": (i, [p, p, p, p, p, d, d, i, p, p, p]),
+            "bnb_holonomic_velocity": (i, [p, p, p, p, p]),
+            "bnb_langevin_half": (i, [i, i, i, p, p, p, p, p, p, p, p, p, d, d, d, d, d, C.c_ulonglong,
+                                      C.c_ulonglong, p, p, p, p]),
             "bnb_set_pme": (i, [p, i, f, p, p]),
             "bnb_pme_grid": (i, [p, i, p]),
             "bnb_compute_pme": (i, [p, p, p, p, i, p, p]),

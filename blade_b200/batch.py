@@ -8,9 +8,14 @@ A step (the same for the batched and the one-at-a-time runs) is
   Langevin VRORV update of coordinates and theta (bnb_langevin_vrorv),
   theta -> lambda (bnb_lambda_from_theta),
 mirroring Run::dynamics (src/run/run.cu:554-564) and State::update
-(src/update/update.cu:233-305) without PME reciprocal, angles/dihedrals and
-constraints; the bonds (TIP3P O-H and H-H included) stand in for the
-reference's bonded terms and SHAKE and keep molecules whole.  All replicas share one libbnb handle, so every kernel of a step
+(src/update/update.cu:233-305) without PME reciprocal and angles/dihedrals;
+the bonds (TIP3P O-H and H-H included) stand in for the reference's bonded
+terms and keep molecules whole.  With ``constraints=True`` the waters are
+rigid instead (holonomic triangles, src/holonomic/holonomic.cu): the update
+is split at its middle (bnb_langevin_half) and bnb_holonomic_position follows
+each half drift, as update_VVhbpR / holonomic_position / update_OOhbpR /
+holonomic_position do (update.cu:276-303), with true hydrogen masses and
+the water bonds dropped.  All replicas share one libbnb handle, so every kernel of a step
 covers all of them; ``capture`` records ``rebuild_every`` steps in one CUDA
 graph that is replayed.  Units are AKMA; dt is 2 fs.
 """
@@ -21,7 +26,7 @@ import math
 
 import numpy as np
 
-from . import _lib
+from . import _lib, holonomic
 from .nbdirect import NbDirect
 from . import systems
 from .systems import System
@@ -33,15 +38,24 @@ PICOSECOND = 20.454828284385908  # AKMA time units per ps (defines.h:51)
 # coordinates' drift per list period within the pad.
 MASS_H, MASS_O, MASS_HEAVY = 3.024, 15.9994 - 2 * (3.024 - 1.008), 12.011
 THETA_MASS = 12.0                # amu A^2, the usual MSLD theta mass
+SHAKE_TOL, SHAKE_ITERS = 1e-10, 10  # FP64 state; the reference's FP32-era default is 2e-7 (run.cu:64)
 
 
-def atom_masses(s: System) -> np.ndarray:
-    """Water H/O by type index (0 = HT, 1 = OT in the generators), heavy atoms otherwise."""
+def atom_masses(s: System, repartition: bool = True) -> np.ndarray:
+    """Water H/O by type index (0 = HT, 1 = OT in the generators), heavy atoms
+    otherwise; hydrogen mass repartitioning unless ``repartition`` is false."""
     t = s.nbonds["typeIdx"]
     m = np.full(s.N, MASS_HEAVY)
-    m[t == 0] = MASS_H
-    m[t == 1] = MASS_O
+    m[t == 0] = MASS_H if repartition else 1.008
+    m[t == 1] = MASS_O if repartition else 15.9994
     return m
+
+
+def water_oxygens(s: System) -> np.ndarray:
+    """First atom of every O, H, H water (types 1, 0, 0 in the generators)."""
+    t = s.nbonds["typeIdx"]
+    i = np.nonzero(t[:-2] == 1)[0]
+    return i[(t[i + 1] == 0) & (t[i + 2] == 0)]
 
 
 def _p(t):
@@ -53,7 +67,7 @@ class MsldBatch:
 
     def __init__(self, reps: list[System], dt_fs: float = 2.0, T: float = 300.0, gamma_ps: float = 1.0,
                  seed: int = 1, rebuild_every: int = 10, energy_every: int = 10, device="cuda", tune=False,
-                 theta_mass: float = THETA_MASS, gamma_theta_ps: float | None = None):
+                 theta_mass: float = THETA_MASS, gamma_theta_ps: float | None = None, constraints: bool = False):
         import torch
         self.torch = torch
         self.reps = reps
@@ -68,18 +82,31 @@ class MsldBatch:
         x = np.concatenate([s.xyz.astype(np.float64) for s in reps]).reshape(-1)
         self.x = torch.from_numpy(x).to(self.dev)
         self.xf = self.x.float()
-        masses = np.concatenate([atom_masses(s) for s in reps])
+        masses = np.concatenate([atom_masses(s, repartition=not constraints) for s in reps])
         rng = np.random.default_rng(seed)
         kT = KB * T
         vx = rng.normal(size=(N, 3)) * np.sqrt(kT / masses)[:, None]
         self.v = torch.from_numpy(vx.reshape(-1)).to(self.dev)
         self.ismx = torch.from_numpy(np.repeat(1 / np.sqrt(masses), 3)).to(self.dev)
         self.force = torch.zeros(3 * N, dtype=f64, device=self.dev)
-        bonds, prm = [], []
+        bonds, prm, tri = [], [], []
         for r, s in enumerate(reps):
-            if s.bonds is not None and len(s.bonds):
-                bonds.append(s.bonds.astype(np.int64) + self.nb.starts[r])
-                prm.append(s.bond_param)
+            keep = np.ones(0 if s.bonds is None else len(s.bonds), bool)
+            if constraints:
+                ox = water_oxygens(s)
+                tri.append(holonomic.water_triangles(0, len(ox)))
+                tri[-1]["idx"] = (ox[:, None] + np.arange(3)[None, :] + int(self.nb.starts[r])).astype(np.int32)
+                wat = np.zeros(s.N, bool)
+                wat[(ox[:, None] + np.arange(3)).reshape(-1)] = True
+                if s.bonds is not None and len(s.bonds):
+                    keep = ~(wat[s.bonds[:, 0]] & wat[s.bonds[:, 1]])
+            if s.bonds is not None and keep.any():
+                bonds.append(s.bonds[keep].astype(np.int64) + self.nb.starts[r])
+                prm.append(s.bond_param[keep])
+        self.cons = holonomic.Constraints(tri=np.concatenate(tri), device=self.dev) if constraints else None
+        self.x_prev = torch.zeros(3 * N, dtype=f64, device=self.dev) if constraints else None
+        self.cons_status = torch.zeros(1, dtype=i32, device=self.dev)
+        self.cons_tol, self.cons_iters = SHAKE_TOL, SHAKE_ITERS
         self.bond_start = None
         if bonds:
             st, pa, pr = systems.bond_csr(N, np.concatenate(bonds), np.concatenate(prm))
@@ -134,6 +161,8 @@ class MsldBatch:
         self.fric_t = at                                  # theta friction (Msld gamma, msld.cu:46, 232-235)
         self.noise_t = math.sqrt((1 - at * at) * kT)
         self._lambda_from_theta()
+        if self.cons is not None:                          # start on the constraint surface
+            self.cons.velocity(self.x, self.v, self.ismx)
         self.fixed_bias = None                             # lambda biases (set_bias)
         self.var_bias = None
         self.hist1 = None                                  # lambda histograms (enable_histograms)
@@ -167,10 +196,21 @@ class MsldBatch:
         self.tforce.zero_()
         _lib.call("bnb_theta_force", self.lambda_site.numel(), _p(self.lambda_site), _p(self.site_bound),
                   float(self.fnex), _p(self.lam), _p(self.theta), _p(self.lforce), _p(self.fixed), _p(self.tforce), s)
-        _lib.call("bnb_langevin_vrorv", self.x.numel(), self.theta.numel(), _p(self.x), _p(self.v), _p(self.force),
-                  _p(self.ismx), _p(self.theta), _p(self.vt), _p(self.tforce), _p(self.ismt), self.dt, self.fric,
-                  self.noise, self.fric_t, self.noise_t, C.c_ulonglong(self.seed), C.c_ulonglong(0),
-                  _p(self.step_counter), _p(self.xf), _p(self.nan), s)
+        if self.cons is None:
+            _lib.call("bnb_langevin_vrorv", self.x.numel(), self.theta.numel(), _p(self.x), _p(self.v),
+                      _p(self.force), _p(self.ismx), _p(self.theta), _p(self.vt), _p(self.tforce), _p(self.ismt),
+                      self.dt, self.fric, self.noise, self.fric_t, self.noise_t, C.c_ulonglong(self.seed),
+                      C.c_ulonglong(0), _p(self.step_counter), _p(self.xf), _p(self.nan), s)
+        else:
+            for phase in (0, 1):                           # VV+R, constrain, OO+R, constrain (update.cu:276-303)
+                _lib.call("bnb_langevin_half", phase, self.x.numel(), self.theta.numel(), _p(self.x), _p(self.v),
+                          _p(self.x_prev), _p(self.force), _p(self.ismx), _p(self.theta), _p(self.vt),
+                          _p(self.tforce), _p(self.ismt), self.dt, self.fric, self.noise, self.fric_t, self.noise_t,
+                          C.c_ulonglong(self.seed), C.c_ulonglong(0), _p(self.step_counter), _p(self.xf),
+                          _p(self.nan), s)
+                self.cons.position(self.x_prev, self.x, self.v, self.ismx, 0.5 * self.dt, self.cons_tol,
+                                   self.cons_iters, x_f=self.xf, status=self.cons_status,
+                                   stream=stream)
         _lib.call("bnb_lambda_from_theta", self.site_bound.numel() - 1, _p(self.site_bound), float(self.fnex),
                   _p(self.theta), _p(self.fixed), _p(self.lam), _p(self.lamf), s)
         if self.hist1 is not None:

@@ -80,6 +80,59 @@ __global__ void k_vrorv(int nx, int nt, double *x, double *v, const double *fx, 
   }
 }
 
+// The same step split at the middle for holonomic constraints, which act
+// after each half drift (update_VVhbpR / update_OOhbpR, update.cu:276-303):
+//   phase 0:  v -= dt ism^2 dU/dx;  xPrev = x;  x += dt/2 v
+//   phase 1:  v = a v + b ism xi;   xPrev = x;  x += dt/2 v
+// Without constraints the two phases give the bits of k_vrorv (same
+// operations in the same order, same noise index); phase 1 advances the
+// device step counter.
+__global__ void k_langevin_half(int phase, int nx, int nt, double *x, double *v, double *xPrev, const double *fx,
+                                const double *ismx, double *th, double *vt, const double *ft, const double *ismt,
+                                double dt, double ax, double bx, double at, double bt, uint64_t seed, uint64_t step,
+                                unsigned long long *stepCounter, float *x_f, int *nanFlag) {
+  __shared__ bool lastBlock;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (stepCounter) step += stepCounter[0];
+  if (i < nx + nt) {
+    const bool spatial = i < nx;
+    const int k = spatial ? i : i - nx;
+    double *X = spatial ? x : th;
+    double *V = spatial ? v : vt;
+    const double ism = spatial ? ismx[k] : ismt[k];
+    double xv = X[k];
+    if (spatial && xPrev) xPrev[k] = xv;
+    if (isfinite(ism)) {
+      double vv = V[k];
+      if (phase == 0) {
+        vv -= dt * ism * ism * (spatial ? fx[k] : ft[k]);
+      } else {
+        const double a = spatial ? ax : at, b = spatial ? bx : bt;
+        vv = a * vv + b * ism * gaussian(seed, step, (uint64_t)i);
+      }
+      xv += 0.5 * dt * vv;
+      V[k] = vv;
+      X[k] = xv;
+      if (!isfinite(vv) && nanFlag) atomicMax(nanFlag, 1);
+    }
+    if (spatial && x_f && phase == 1) x_f[k] = (float)xv;
+  }
+  if (stepCounter && phase == 1) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      unsigned long long done = atomicAdd(&stepCounter[1], 1ull);
+      lastBlock = done == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (lastBlock && threadIdx.x == 0) {
+      stepCounter[1] = 0;
+      __threadfence();
+      atomicAdd(&stepCounter[0], 1ull);
+    }
+  }
+}
+
 // Harmonic bonds, gathered per atom: thread a walks its own CSR row of bond
 // partners in stored order and adds sum_b kb (r - b0) (x_a - x_b) / r to
 // grad[a] -- each bond is evaluated from both ends, which keeps the sum
@@ -129,5 +182,23 @@ extern "C" int bnb_langevin_vrorv(int nx, int nt, double *x, double *v, const do
   k_vrorv<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(nx, nt, x, v, fx, ismx, theta, vtheta, ftheta,
                                                              ismtheta, dt, frictionX, noiseX, frictionTheta,
                                                              noiseTheta, seed, step, stepCounter, x_f, nanFlag);
+  return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
+}
+
+extern "C" int bnb_langevin_half(int phase, int nx, int nt, double *x, double *v, double *xPrev, const double *fx,
+                                 const double *ismx, double *theta, double *vtheta, const double *ftheta,
+                                 const double *ismtheta, double dt, double frictionX, double noiseX,
+                                 double frictionTheta, double noiseTheta, unsigned long long seed,
+                                 unsigned long long step, unsigned long long *stepCounter, float *x_f,
+                                 int *nanFlag, void *stream) {
+  if ((phase != 0 && phase != 1) || nx < 0 || nt < 0 || (nx > 0 && (!x || !v || !ismx || (phase == 0 && !fx))) ||
+      (nt > 0 && (!theta || !vtheta || !ismtheta || (phase == 0 && !ftheta))))
+    return BNB_ERR_ARG;
+  int n = nx + nt;
+  if (n == 0) return BNB_OK;
+  k_langevin_half<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(phase, nx, nt, x, v, xPrev, fx, ismx, theta,
+                                                                     vtheta, ftheta, ismtheta, dt, frictionX, noiseX,
+                                                                     frictionTheta, noiseTheta, seed, step,
+                                                                     stepCounter, x_f, nanFlag);
   return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
 }

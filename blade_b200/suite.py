@@ -197,7 +197,7 @@ def run_batch(args):
     atoms = [r.N for r in reps]
     K = args.steps
     # batched: one handle, autotuned, one CUDA graph per 10 steps
-    B = MsldBatch(reps, tune=True)
+    B = MsldBatch(reps, tune=True, constraints=args.constraints)
     tuning = B.tuning()
     B.capture()
     B.run_graph(20)
@@ -233,7 +233,7 @@ def run_batch(args):
     t_seq_graph = 0.0
     bad = 0
     for r in reps:
-        S = MsldBatch([r], tune=args.tune_sequential)
+        S = MsldBatch([r], tune=args.tune_sequential, constraints=args.constraints)
         S.run_eager(10)
         torch.cuda.synchronize()
         a, b = _events()
@@ -256,8 +256,10 @@ def run_batch(args):
     line = {"config": f"{R} MSLD replicas, 3k-30k atoms (log-uniform), 1-3 sites x 2-5 substituents, "
                       "rCut 12, PME+VFSWITCH, soft core, dt 2 fs",
             "replicas": R, "atoms_total": int(sum(atoms)), "atoms_min": min(atoms), "atoms_max": max(atoms),
-            "steps": K, "step": "rebuild/10 + nbdirect(MSLD) + dU/dlambda->dU/dtheta + Langevin VRORV(x, theta) "
-                                "+ harmonic bonds + theta->lambda; no PME recip, angles, dihedrals or SHAKE",
+            "steps": K, "step": ("rebuild/10 + nbdirect(MSLD) + dU/dlambda->dU/dtheta + Langevin VRORV(x, theta) "
+                                 + ("split around holonomic constraints (rigid TIP3P, true H masses) + chain bonds"
+                                    if args.constraints else "+ harmonic bonds (HMR)")
+                                 + " + theta->lambda; no PME recip, angles or dihedrals"),
             "batched_graph": {"seconds": t_batch, "ns_per_day_aggregate": ns_per_day(K, t_batch, replicas=R),
                               "tuning": tuning, "status": st, "nan": nan, "breakdown": breakdown},
             "sequential_eager": {"seconds": t_seq, "ns_per_day_aggregate": ns_per_day(K, t_seq, replicas=R)},
@@ -409,6 +411,7 @@ def main(argv=None):
     ap.add_argument("--eval-modes", default="plain,learned:1")
     ap.add_argument("--target", default="flat", choices=["flat", "lookahead"])
     ap.add_argument("--parts", default="single,batch", help="pme: single (one system) and/or batch")
+    ap.add_argument("--constraints", action="store_true", help="batch: rigid waters (holonomic constraints)")
     args, rest = ap.parse_known_args(argv)
     if args.what in ("msld", "water"):
         run_msld(args, water_only=args.what == "water")

@@ -394,6 +394,56 @@ int bnb_langevin_vrorv(int nx, int nt, double *x, double *v, const double *fx,
                        unsigned long long step, unsigned long long *stepCounter,
                        float *x_f, int *nanFlag, void *stream);
 
+/*
+ * The Langevin step split at its middle for holonomic constraints
+ * (update_VVhbpR / update_OOhbpR, src/update/update.cu:276-303): phase 0
+ * kicks and drifts half a step, phase 1 applies friction and noise and drifts
+ * the other half; each phase first copies x to xPrev (device double [nx],
+ * may be NULL without constraints), and bnb_holonomic_position follows each
+ * phase.  Arguments as bnb_langevin_vrorv; without constraints phase 0 then
+ * phase 1 equals one bnb_langevin_vrorv bit for bit.  x_f is written by
+ * phase 1 (and by bnb_holonomic_position for constrained atoms).
+ */
+int bnb_langevin_half(int phase, int nx, int nt, double *x, double *v, double *xPrev, const double *fx,
+                      const double *ismx, double *theta, double *vtheta, const double *ftheta,
+                      const double *ismtheta, double dt, double frictionX, double noiseX,
+                      double frictionTheta, double noiseTheta, unsigned long long seed,
+                      unsigned long long step, unsigned long long *stepCounter, float *x_f,
+                      int *nanFlag, void *stream);
+
+/*
+ * Holonomic bond constraints (holonomic_position / holonomic_velocity,
+ * src/holonomic/holonomic.cu:238-758).  The cluster layouts are the
+ * reference's TriangleCons / Branch1Cons / Branch2Cons / Branch3Cons
+ * (src/system/potential.h:120-138): a rigid triangle with b0 = |01|, |02|,
+ * |12|, or a heavy atom (idx[0]) with 1-3 hydrogens, b0[k] = |0 (k+1)|;
+ * every atom in at most one cluster; device arrays.
+ * bnb_holonomic_position corrects the drifted positions x (device double
+ * [3N]) along the bond vectors of xPrev until |b0^2 - r^2| < 2 b0^2 tolerance
+ * (Run::shakeTolerance) or maxIter iterations (then status bit 1 is set, if
+ * status is given), and sets v = (x - xPrev) / halfdt for the cluster atoms
+ * (v may be NULL).  ism: device double [3N], 1/sqrt(m) per degree of freedom
+ * (LeapState::ism).  x_f (optional): FP32 copy of the constrained positions.
+ * bnb_holonomic_velocity removes the bond-direction relative velocities.
+ * Coordinates must be unwrapped: a cluster is not split across images.
+ */
+typedef struct { int idx[3]; float b0[3]; } bnb_triangle_cons;
+typedef struct { int idx[2]; float b0[1]; } bnb_branch1_cons;
+typedef struct { int idx[3]; float b0[2]; } bnb_branch2_cons;
+typedef struct { int idx[4]; float b0[3]; } bnb_branch3_cons;
+typedef struct {
+  int nTriangle, nBranch1, nBranch2, nBranch3;
+  const bnb_triangle_cons *triangle;
+  const bnb_branch1_cons *branch1;
+  const bnb_branch2_cons *branch2;
+  const bnb_branch3_cons *branch3;
+} bnb_constraints;
+int bnb_holonomic_position(const bnb_constraints *cs, const double *xPrev, double *x, double *v,
+                           const double *ism, double halfdt, double tolerance, int maxIter,
+                           float *x_f, int *status, void *stream);
+int bnb_holonomic_velocity(const bnb_constraints *cs, const double *x, double *v, const double *ism,
+                           void *stream);
+
 /* Library version string. */
 /* ---- BF16 MLP of learned landscape flattening (no reference counterpart;
  * BLaDE's src/mlp is TorchANI inference, unrelated).  Row-major arrays,

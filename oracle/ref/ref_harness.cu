@@ -15,7 +15,9 @@
 // src/system/potential.cxx:1839-1929), on one stream; ref_evaluate_pairs
 // calls getforce_nb14 / getforce_nbex (src/bonded/pair.cu) the same way, and
 // ref_evaluate_pme getforce_ewald / getforce_ewaldself (src/nbrecip/nbrecip.cu)
-// on PME grids set up as Potential::initialize does (potential.cxx:1202-1300).
+// on PME grids set up as Potential::initialize does (potential.cxx:1202-1300),
+// and ref_holonomic holonomic_position / holonomic_velocity
+// (src/holonomic/holonomic.cu) on given constraint clusters.
 #include <cuda_runtime.h>
 #include <cufft.h>
 
@@ -33,6 +35,7 @@
 #include "msld/msld.h"
 #include "nbdirect/nbdirect.h"
 #include "nbrecip/nbrecip.h"
+#include "holonomic/holonomic.h"
 #include "run/run.h"
 #include "system/potential.h"
 #include "system/state.h"
@@ -438,4 +441,71 @@ extern "C" int ref_time_pme(ref_handle *h, int reps, int energyEvery, double *ms
   }
   *ms = total;
   return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// Constraint clusters in the layouts of TriangleCons / Branch1Cons /
+// Branch2Cons / Branch3Cons (host arrays); xPrev, x: host double [3N];
+// ism: host float [3N] (LeapState::ism); v: host float [3N] in/out.
+// which 0: holonomic_position (x corrected, v from the displacement);
+// which 1: holonomic_velocity (v projected, x unchanged).
+extern "C" int ref_holonomic(ref_handle *h, int which, int nTri, const void *tri, int n1, const void *b1, int n2,
+                             const void *b2, int n3, const void *b3, const double *xPrev, double *x, float *v,
+                             const float *ism, float halfdt, float tolerance) {
+  System *sys = h->sys;
+  Potential *pot = h->pot;
+  State *st = h->st;
+  const int N = h->N;
+  pot->triangleConsCount = nTri;
+  pot->branch1ConsCount = n1;
+  pot->branch2ConsCount = n2;
+  pot->branch3ConsCount = n3;
+  cudaMalloc(&pot->triangleCons_d, sizeof(TriangleCons) * (nTri > 0 ? nTri : 1));
+  cudaMalloc(&pot->branch1Cons_d, sizeof(Branch1Cons) * (n1 > 0 ? n1 : 1));
+  cudaMalloc(&pot->branch2Cons_d, sizeof(Branch2Cons) * (n2 > 0 ? n2 : 1));
+  cudaMalloc(&pot->branch3Cons_d, sizeof(Branch3Cons) * (n3 > 0 ? n3 : 1));
+  if (nTri) cudaMemcpy(pot->triangleCons_d, tri, sizeof(TriangleCons) * nTri, cudaMemcpyHostToDevice);
+  if (n1) cudaMemcpy(pot->branch1Cons_d, b1, sizeof(Branch1Cons) * n1, cudaMemcpyHostToDevice);
+  if (n2) cudaMemcpy(pot->branch2Cons_d, b2, sizeof(Branch2Cons) * n2, cudaMemcpyHostToDevice);
+  if (n3) cudaMemcpy(pot->branch3Cons_d, b3, sizeof(Branch3Cons) * n3, cudaMemcpyHostToDevice);
+  h->run->shakeTolerance = tolerance;
+  double *x_d, *xp_d;
+  float *v_d, *ism_d;
+  cudaMalloc(&x_d, sizeof(double) * 3 * N);
+  cudaMalloc(&xp_d, sizeof(double) * 3 * N);
+  cudaMalloc(&v_d, sizeof(float) * 3 * N);
+  cudaMalloc(&ism_d, sizeof(float) * 3 * N);
+  cudaMemcpy(x_d, x, sizeof(double) * 3 * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(xp_d, xPrev, sizeof(double) * 3 * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(v_d, v, sizeof(float) * 3 * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(ism_d, ism, sizeof(float) * 3 * N, cudaMemcpyHostToDevice);
+  LeapState ls;
+  memset(&ls, 0, sizeof(ls));
+  ls.N1 = 3 * N;
+  ls.N = 3 * N;
+  ls.x = x_d;
+  ls.v = v_d;
+  ls.ism = ism_d;
+  LeapParms2 lp;
+  memset(&lp, 0, sizeof(lp));
+  lp.halfdt = halfdt;
+  st->leapState = &ls;
+  st->leapParms2 = &lp;
+  st->positionCons_d = xp_d;
+  if (which == 0) holonomic_position(sys);
+  else holonomic_velocity(sys);
+  int rc = cudaStreamSynchronize(h->stream) == cudaSuccess ? 0 : 2;
+  cudaMemcpy(x, x_d, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost);
+  cudaMemcpy(v, v_d, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost);
+  st->leapState = NULL;
+  st->leapParms2 = NULL;
+  st->positionCons_d = NULL;
+  cudaFree(x_d);
+  cudaFree(xp_d);
+  cudaFree(v_d);
+  cudaFree(ism_d);
+  cudaFree(pot->triangleCons_d);
+  cudaFree(pot->branch1Cons_d);
+  cudaFree(pot->branch2Cons_d);
+  cudaFree(pot->branch3Cons_d);
+  return rc ? rc : (cudaGetLastError() == cudaSuccess ? 0 : 2);
 }

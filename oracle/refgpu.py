@@ -33,6 +33,7 @@ def lib():
         L.ref_set_pme.argtypes = [p, i, p, p, p]
         L.ref_evaluate_pme.argtypes = [p, i, i, p, p, p]
         L.ref_time_pme.argtypes = [p, i, i, p]
+        L.ref_holonomic.argtypes = [p, i, i, p, i, p, i, p, i, p, p, p, p, p, f, f]
         _lib = L
     return _lib
 
@@ -138,3 +139,32 @@ class RefGPU:
         if rc != 0:
             raise RuntimeError("reference harness: timing failed")
         return ms.value
+
+
+def holonomic(which, tri, b1, b2, b3, x_prev, x, v, ism, halfdt, tolerance):
+    """The reference's holonomic_position (which="position") or
+    holonomic_velocity (which="velocity") on the given clusters
+    (TriangleCons / Branch*Cons layouts) and state; returns (x, v) with the
+    reference's precisions (x double, v and ism float)."""
+    N = len(x_prev)
+    P = lambda a: a.ctypes.data_as(C.c_void_p)
+    z = np.zeros(N, np.int32)
+    zf = np.zeros(N, np.float32)
+    vdw = np.zeros(2, np.float32)
+    box = np.full(3, 100.0)
+    h = C.c_void_p()
+    if lib().ref_create(N, P(z), P(zf), P(z), 1, P(vdw), 0, None, 1, 0, 9.0, 8.0, 0.34, 1, 0, 2.0, P(box),
+                        C.byref(h)) != 0:
+        raise RuntimeError("reference harness: create failed")
+    xp = np.ascontiguousarray(x_prev, np.float64).reshape(-1)
+    xo = np.ascontiguousarray(x, np.float64).reshape(-1).copy()
+    vo = np.ascontiguousarray(v, np.float32).reshape(-1).copy()
+    im = np.ascontiguousarray(ism, np.float32).reshape(-1)
+    arrs = [np.ascontiguousarray(a) for a in (tri, b1, b2, b3)]
+    ptr = lambda a: P(a) if len(a) else None
+    rc = lib().ref_holonomic(h, 0 if which == "position" else 1, len(arrs[0]), ptr(arrs[0]), len(arrs[1]),
+                             ptr(arrs[1]), len(arrs[2]), ptr(arrs[2]), len(arrs[3]), ptr(arrs[3]), P(xp), P(xo),
+                             P(vo), P(im), float(halfdt), float(tolerance))
+    if rc != 0:
+        raise RuntimeError("reference harness: holonomic failed")
+    return xo.reshape(-1, 3), vo.reshape(-1, 3)

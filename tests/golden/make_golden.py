@@ -16,7 +16,10 @@ combinations, PME exclusion corrections) and the MSLD water box; and, from
 the reference's getforce_ewald / getforce_ewaldself (src/nbrecip/nbrecip.cu),
 pme_*.npz: reciprocal-space dU/dx, energy and dU/dlambda plus the self term
 for the water box (orders 4, 6, 8), the MSLD water box and a small
-chain-in-water system (--pme-only makes just these).
+chain-in-water system (--pme-only makes just these); and, from the
+reference's holonomic_position / holonomic_velocity
+(src/holonomic/holonomic.cu), holonomic_*.npz for rigid waters and
+X-H groups of one to three hydrogens (--holonomic-only makes just these).
 """
 import os
 import sys
@@ -70,8 +73,25 @@ def pme_cases():
     yield "pme_chain_small", s, 6, [pme_oracle.grid_size(L, 1.0) for L in s.box]
 
 
-def main(out, pairs_only=False, pme_only=False):
+def holonomic_cases(out):
+    from oracle import holonomic_oracle as H
+    for name, jitter in (("holonomic_small_drift", 0.01), ("holonomic_large_drift", 0.05)):
+        T, B1, B2, B3, xp, x, ism = H.test_clusters(seed=3, jitter=jitter)
+        halfdt = 0.5 * 0.002 / 4.88882129e-02  # 2 fs in AKMA time units
+        xr, vr = refgpu.holonomic("position", T, B1, B2, B3, xp, x, np.zeros_like(x), ism, halfdt, 1e-10)
+        v_in = np.random.default_rng(4).normal(0, 5, x.shape)
+        _, vv = refgpu.holonomic("velocity", T, B1, B2, B3, xp, xr, v_in, ism, halfdt, 1e-10)
+        np.savez_compressed(os.path.join(out, name + ".npz"), x_prev=xp, x=x, ism=ism, halfdt=np.float64(halfdt),
+                            tri=T.view(np.uint8), b1=B1.view(np.uint8), b2=B2.view(np.uint8), b3=B3.view(np.uint8),
+                            x_ref=xr, v_ref=vr.astype(np.float32), v_in=v_in, v_proj_ref=vv.astype(np.float32))
+        print(name, len(T), len(B1), len(B2), len(B3), flush=True)
+
+
+def main(out, pairs_only=False, pme_only=False, holonomic_only=False):
     os.makedirs(out, exist_ok=True)
+    if holonomic_only:
+        holonomic_cases(out)
+        return
     for name, s, order, K in pme_cases():
         ref = refgpu.RefGPU(s)
         ref.set_pme(order, K)
@@ -109,4 +129,4 @@ def main(out, pairs_only=False, pme_only=False):
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     main(args[0] if args else os.path.join(ROOT, "golden_out"), pairs_only="--pairs-only" in sys.argv,
-         pme_only="--pme-only" in sys.argv)
+         pme_only="--pme-only" in sys.argv, holonomic_only="--holonomic-only" in sys.argv)
