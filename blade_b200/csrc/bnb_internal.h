@@ -88,7 +88,7 @@ struct Dev {
   float *slotQ;            // [32*maxBlocks]
   int *slotType;           // [32*maxBlocks]
   int *slotSiteBlock;      // [32*maxBlocks]
-  float4 *colMin, *colMax; // [totalCols] union of the column's block AABBs (cull pre-test)
+  uint32_t *colKey;        // [6*totalCols] column AABB (union of its blocks) as order-preserving keys
   int *exclBlk;            // [maxBlocks*kExclBlk] distinct blocks holding excluded partners
   int *exclBlkCount;       // [maxBlocks] entries in exclBlk, -1 = more than kExclBlk
   int *cullCount;          // [maxBlocks*kNumShifts]

@@ -188,7 +188,7 @@ int alloc_list(bnb_handle *h) {
   size_t o_bb = a.take<int>(MB + 1), o_brep = a.take<int>(MB), o_rbs = a.take<int>(h->R + 1);
   size_t o_slotA = a.take<int>(32 * MB), o_atomSlot = a.take<int>(N), o_slotQ = a.take<float>(32 * MB),
          o_slotT = a.take<int>(32 * MB), o_slotSB = a.take<int>(32 * MB);
-  size_t o_cmin = a.take<float4>(C), o_cmax = a.take<float4>(C), o_eb = a.take<int>(bnb::kExclBlk * MB),
+  size_t o_ckey = a.take<uint32_t>(6 * (size_t)C), o_eb = a.take<int>(bnb::kExclBlk * MB),
          o_ebc = a.take<int>(MB);
   size_t o_cullC = a.take<int>(MB * bnb::kNumShifts), o_cullO = a.take<int>(MB * bnb::kNumShifts + 1);
   size_t o_cand = a.take<int4>(h->capCand), o_cflag = a.take<int>(h->capCand),
@@ -222,8 +222,7 @@ int alloc_list(bnb_handle *h) {
   d.slotQ = (float *)(b + o_slotQ);
   d.slotType = (int *)(b + o_slotT);
   d.slotSiteBlock = (int *)(b + o_slotSB);
-  d.colMin = (float4 *)(b + o_cmin);
-  d.colMax = (float4 *)(b + o_cmax);
+  d.colKey = (uint32_t *)(b + o_ckey);
   d.exclBlk = (int *)(b + o_eb);
   d.exclBlkCount = (int *)(b + o_ebc);
   d.cullCount = (int *)(b + o_cullC);
@@ -313,10 +312,6 @@ int upload_rep(bnb_handle *h, cudaStream_t s) {
                             cudaMemcpyHostToDevice, s))
              ? BNB_OK
              : BNB_ERR_CUDA;
-}
-
-__global__ void k_clear_list_status(bnb::Counters *c) {
-  atomicAnd(&c->status, ~bnb::kStatusListInvalid);
 }
 
 }  // namespace
@@ -596,8 +591,7 @@ int bnb_rebuild(bnb_handle *h, const float *position, const float *boxes, void *
   for (int attempt = 0; attempt < 12; attempt++) {
     const bool rec = h->prof && h->rebN < kProfSlots;
     if (rec) cudaEventRecord(h->rebEv[2 * h->rebN], s);
-    k_clear_list_status<<<1, 1, 0, s>>>(h->d.ctr);
-    h->launches += 1 + bnb::rebuild_list(h->d, h->colRep_d, position, rcull2, s);
+    h->launches += bnb::rebuild_list(h->d, h->colRep_d, position, rcull2, s);
     if (rec) cudaEventRecord(h->rebEv[2 * h->rebN++ + 1], s);
     if (!ok(cudaGetLastError())) return BNB_ERR_CUDA;
     if (async) {

@@ -149,15 +149,48 @@ __global__ void k_scan_down(const int *in, int *out, int n, const int *partial) 
   }
 }
 
+// Small arrays: one CTA walks the array tile by tile with a running carry.
+__global__ void k_scan_single(const int *in, int *out, int n, int *total) {
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < n; base += kScanTile) {
+    const int first = base + threadIdx.x * kScanItems;
+    int v[kScanItems];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+      v[k] = first + k < n ? in[first + k] : 0;
+      sum += v[k];
+    }
+    int tot;
+    int off = block_excl_scan(sum, &tot) + carry;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+      if (first + k < n) out[first + k] = off;
+      off += v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && total) *total = carry;
+}
+
 }  // namespace
 
-void scan_exclusive(const int *in, int *out, int n, int *total, int *partial,
-                    cudaStream_t s) {
+int scan_exclusive(const int *in, int *out, int n, int *total, int *partial,
+                   cudaStream_t s) {
+  if (n <= 4 * kScanTile) {  // up to 16,384 items: one launch instead of three
+    k_scan_single<<<1, kScanThreads, 0, s>>>(in, out, n, total);
+    return 1;
+  }
   int parts = (n + kScanTile - 1) / kScanTile;
   if (parts < 1) parts = 1;
   k_scan_reduce<<<parts, kScanThreads, 0, s>>>(in, n, partial);
   k_scan_top<<<1, kScanThreads, 0, s>>>(partial, parts, total);
   k_scan_down<<<parts, kScanThreads, 0, s>>>(in, out, n, partial);
+  return 3;
 }
 
 namespace {
@@ -167,6 +200,7 @@ namespace {
 // ---------------------------------------------------------------------------
 __global__ void k_bin(Dev d, const float *__restrict__ pos) {
   int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a == 0) atomicAnd(&d.ctr->status, ~kStatusListInvalid);  // this rebuild starts a fresh list
   if (a >= d.N) return;
   const RepInfo ri = d.rep[d.atomRep[a]];
   float w[3];
@@ -233,6 +267,11 @@ __global__ void k_colscan(Dev d, const int *__restrict__ colRep) {
       d.colStartAtom[c] = offA;
       d.colStartBlock[c] = offB;
       d.colFill[c] = 0;
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        d.colKey[6 * c + k] = 0xFFFFFFFFu;  // min keys: larger than any value
+        d.colKey[6 * c + 3 + k] = 0u;       // max keys: smaller than any value
+      }
       int r = colRep[c];
       for (int k = 0; k < nb; k++) {
         int b = offB + k;
@@ -281,6 +320,8 @@ __global__ void k_colsort(Dev d) {
   const int n = d.colCount[c];
   const int base = d.colStartAtom[c];
   if (n == 0) return;
+  __syncthreads();  // every thread has read the count
+  if (threadIdx.x == 0) d.colCount[c] = 0;  // zero for the next rebuild's binning
   if (n <= kSortCap) {
     int n2 = 1;
     while (n2 < n) n2 <<= 1;
@@ -352,8 +393,12 @@ __global__ void k_slots(Dev d) {
 
 }  // namespace
 
-// 6. Pack coordinates with the stored image shift; per-block AABBs.
-__global__ void k_pack(Dev d, const float *__restrict__ pos) {
+// 6. Pack coordinates with the stored image shift; per-block AABBs.  At a
+//    rebuild (columns) also the column AABBs, the union of the column's block
+//    boxes, by atomic min/max of order-preserving keys (order-independent, so
+//    reproducible).  A block that hits implies its column hits under the
+//    rounding of aabb_hit, so the cull may skip columns that miss.
+__global__ void k_pack(Dev d, const float *__restrict__ pos, bool columns) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   int b = t >> 5;
   if (b >= d.maxBlocks) return;
@@ -386,42 +431,22 @@ __global__ void k_pack(Dev d, const float *__restrict__ pos) {
   if ((t & 31) == 0) {
     d.bmin[b] = make_float4(mn.x, mn.y, mn.z, 0.f);
     d.bmax[b] = make_float4(mx.x, mx.y, mx.z, 0.f);
+    if (columns) {
+      unsigned *key = d.colKey + 6 * d.atomCol[a];  // lane 0 of a block always holds an atom
+      atomicMin(key + 0, z_key(mn.x));
+      atomicMin(key + 1, z_key(mn.y));
+      atomicMin(key + 2, z_key(mn.z));
+      atomicMax(key + 3, z_key(mx.x));
+      atomicMax(key + 4, z_key(mx.y));
+      atomicMax(key + 5, z_key(mx.z));
+    }
   }
 }
 
 namespace {
 
-// 6b. Column AABBs: union of the AABBs of each column's blocks (one warp per
-//     column).  The union contains every member box, so with the rounding of
-//     aabb_hit a block that hits implies its column hits; the cull below may
-//     skip columns that miss without changing the candidate list.
-__global__ void k_colbox(Dev d) {
-  const int lane = threadIdx.x & 31;
-  const int nWarps = (gridDim.x * blockDim.x) >> 5;
-  const int B = d.ctr->blockCount;
-  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < d.totalCols; c += nWarps) {
-    int b0 = d.colStartBlock[c], b1 = d.colStartBlock[c + 1];
-    b1 = b1 < B ? b1 : B;
-    float3 mn = make_float3(INFINITY, INFINITY, INFINITY), mx = make_float3(-INFINITY, -INFINITY, -INFINITY);
-    for (int b = b0 + lane; b < b1; b += 32) {
-      const float4 lo = d.bmin[b], hi = d.bmax[b];
-      mn.x = fminf(mn.x, lo.x); mn.y = fminf(mn.y, lo.y); mn.z = fminf(mn.z, lo.z);
-      mx.x = fmaxf(mx.x, hi.x); mx.y = fmaxf(mx.y, hi.y); mx.z = fmaxf(mx.z, hi.z);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      mn.x = fminf(mn.x, __shfl_xor_sync(kFull, mn.x, o));
-      mn.y = fminf(mn.y, __shfl_xor_sync(kFull, mn.y, o));
-      mn.z = fminf(mn.z, __shfl_xor_sync(kFull, mn.z, o));
-      mx.x = fmaxf(mx.x, __shfl_xor_sync(kFull, mx.x, o));
-      mx.y = fmaxf(mx.y, __shfl_xor_sync(kFull, mx.y, o));
-      mx.z = fmaxf(mx.z, __shfl_xor_sync(kFull, mx.z, o));
-    }
-    if (lane == 0) {
-      d.colMin[c] = make_float4(mn.x, mn.y, mn.z, 0.f);
-      d.colMax[c] = make_float4(mx.x, mx.y, mx.z, 0.f);
-    }
-  }
+__device__ __forceinline__ float key_float(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k ^ 0x80000000u) : ~k);
 }
 
 // 7/9. Cull: one warp per (iBlock, shift code); count pass then write pass.
@@ -440,6 +465,7 @@ __global__ void k_cull(Dev d, float rcull2) {
     int iBlock = gw / kNumShifts, code = gw - iBlock * kNumShifts;
     if (iBlock >= B) {
       if (!kWrite && lane == 0) d.cullCount[gw] = 0;
+      if (kWrite && lane == 0 && code == 0) d.workCountPerBlock[iBlock] = 0;
       continue;
     }
     int r = d.blockRep[iBlock];
@@ -460,7 +486,12 @@ __global__ void k_cull(Dev d, float rcull2) {
         int be = d.colStartBlock[c + 1];
         bs = bs > j0 ? bs : j0;
         be = be < j1 ? be : j1;
-        if (bs < be && aabb_hit(imin, imax, d.colMin[c], d.colMax[c], sh, rcull2)) n = be - bs;
+        if (bs < be) {
+          const uint32_t *key = d.colKey + 6 * c;
+          const float4 cmin = make_float4(key_float(key[0]), key_float(key[1]), key_float(key[2]), 0.f);
+          const float4 cmax = make_float4(key_float(key[3]), key_float(key[4]), key_float(key[5]), 0.f);
+          if (aabb_hit(imin, imax, cmin, cmax, sh, rcull2)) n = be - bs;
+        }
       }
       int inc = n;
 #pragma unroll
@@ -494,29 +525,20 @@ __global__ void k_cull(Dev d, float rcull2) {
       }
     }
     if (!kWrite && lane == 0) d.cullCount[gw] = cnt;
-  }
-}
-
-// Candidate bookkeeping after the cull scan.
-__global__ void k_cand_finish(Dev d) {
-  int total = d.cullOffset[d.maxBlocks * kNumShifts];
-  int B = d.ctr->blockCount;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t == 0) {
-    d.ctr->candCount = total < d.capCand ? total : d.capCand;
-    if (total > d.capCand) atomicOr(&d.ctr->status, kStatusCandOverflow);
-  }
-  for (int b = t; b <= B; b += gridDim.x * blockDim.x) {
-    int s = d.cullOffset[b * kNumShifts];
-    d.candStart[b] = s < d.capCand ? s : d.capCand;
-    if (b < B) {
-      int e = d.cullOffset[(b + 1) * kNumShifts];
-      e = e < d.capCand ? e : d.capCand;
-      s = s < d.capCand ? s : d.capCand;
-      d.workCountPerBlock[b] = (e - s + d.tilesPerWork - 1) / d.tilesPerWork;
+    if (kWrite && lane == 0 && code == 0) {  // candidate range and work items of this i block
+      int c0 = d.cullOffset[gw], c1 = d.cullOffset[gw + kNumShifts];
+      c0 = c0 < d.capCand ? c0 : d.capCand;
+      c1 = c1 < d.capCand ? c1 : d.capCand;
+      d.candStart[iBlock] = c0;
+      d.workCountPerBlock[iBlock] = (c1 - c0 + d.tilesPerWork - 1) / d.tilesPerWork;
     }
   }
-  for (int b = B + t; b < d.maxBlocks; b += gridDim.x * blockDim.x) d.workCountPerBlock[b] = 0;
+  if (kWrite && blockIdx.x == 0 && threadIdx.x == 0) {
+    const int tot = d.cullOffset[d.maxBlocks * kNumShifts];
+    d.ctr->candCount = tot < d.capCand ? tot : d.capCand;
+    if (tot > d.capCand) atomicOr(&d.ctr->status, kStatusCandOverflow);
+    d.candStart[B] = d.ctr->candCount;
+  }
 }
 
 // 10/12. Exclusion rows of a candidate tile: one warp, lane = i atom.
@@ -610,12 +632,11 @@ __global__ void k_excl(Dev d) {
       if (lane == 0) d.cand[c].z = idx;
     }
   }
-}
-
-__global__ void k_mask_finish(Dev d) {
-  int total = d.candMaskOff[d.capCand];
-  d.ctr->maskCount = total < d.capMask ? total : d.capMask;
-  if (total > d.capMask) atomicOr(&d.ctr->status, kStatusMaskOverflow);
+  if (kWrite && blockIdx.x == 0 && threadIdx.x == 0) {
+    const int tot = d.candMaskOff[d.capCand];
+    d.ctr->maskCount = tot < d.capMask ? tot : d.capMask;
+    if (tot > d.capMask) atomicOr(&d.ctr->status, kStatusMaskOverflow);
+  }
 }
 
 // 13. Work items: (iBlock, first candidate) chunks of d.tilesPerWork tiles.
@@ -646,36 +667,42 @@ inline int grid_for(long long n, int threads) {
 
 void pack_positions(const Dev &d, const float *pos, cudaStream_t s) {
   int n = 32 * d.maxBlocks;
-  k_pack<<<grid_for(n, 256), 256, 0, s>>>(d, pos);
+  k_pack<<<grid_for(n, 256), 256, 0, s>>>(d, pos, false);
 }
+
+namespace {
+__global__ void k_clear_status(Counters *c) { atomicAnd(&c->status, ~kStatusListInvalid); }
+}  // namespace
 
 int rebuild_list(const Dev &d, const int *colRep, const float *pos, float rcull2,
                  cudaStream_t s) {
-  cudaMemsetAsync(d.colCount, 0, sizeof(int) * d.totalCols, s);
-  const int launches = (d.N > 0 ? 2 : 0) + 22;
-  if (d.N > 0) k_bin<<<grid_for(d.N, 256), 256, 0, s>>>(d, pos);
+  int launches = 8;  // bin or clear, colscan, colsort, slots, pack, excl_blocks, work, + scatter or not below
+  // colCount is zero here: set so at allocation and by k_colsort after use
+  if (d.N > 0) k_bin<<<grid_for(d.N, 256), 256, 0, s>>>(d, pos);  // also clears the list-invalid bits
+  else k_clear_status<<<1, 1, 0, s>>>(d.ctr);
   k_colscan<<<1, 1024, 0, s>>>(d, colRep);
-  if (d.N > 0) k_scatter<<<grid_for(d.N, 256), 256, 0, s>>>(d);
+  if (d.N > 0) {
+    k_scatter<<<grid_for(d.N, 256), 256, 0, s>>>(d);
+    launches++;
+  }
   k_colsort<<<d.totalCols, 512, 0, s>>>(d);
   k_slots<<<grid_for(32LL * d.maxBlocks, 256), 256, 0, s>>>(d);
-  pack_positions(d, pos, s);
-  k_colbox<<<grid_for(32LL * d.totalCols, 256), 256, 0, s>>>(d);
+  k_pack<<<grid_for(32LL * d.maxBlocks, 256), 256, 0, s>>>(d, pos, true);
   k_excl_blocks<<<grid_for(32LL * d.maxBlocks, 256), 256, 0, s>>>(d);
   // cull: count, scan, write
   const int cullWarps = d.maxBlocks * kNumShifts;
   const int cullGrid = grid_for(32LL * cullWarps, 256) < 148 * 32 ? grid_for(32LL * cullWarps, 256) : 148 * 32;
   k_cull<false><<<cullGrid, 256, 0, s>>>(d, rcull2);
-  scan_exclusive(d.cullCount, d.cullOffset, cullWarps, d.cullOffset + cullWarps, d.scanPartial, s);
-  k_cull<true><<<cullGrid, 256, 0, s>>>(d, rcull2);
-  k_cand_finish<<<grid_for(d.maxBlocks + 1, 256), 256, 0, s>>>(d);
+  launches += 4;  // two cull and two exclusion passes
+  launches += scan_exclusive(d.cullCount, d.cullOffset, cullWarps, d.cullOffset + cullWarps, d.scanPartial, s);
+  k_cull<true><<<cullGrid, 256, 0, s>>>(d, rcull2);  // also candStart, work counts, candCount
   // exclusion masks: flag, scan, write
   const int exGrid = grid_for(32LL * d.capCand, 256) < 148 * 16 ? grid_for(32LL * d.capCand, 256) : 148 * 16;
   k_excl<false><<<exGrid, 256, 0, s>>>(d);
-  scan_exclusive(d.candFlag, d.candMaskOff, d.capCand, d.candMaskOff + d.capCand, d.scanPartial, s);
-  k_excl<true><<<exGrid, 256, 0, s>>>(d);
-  k_mask_finish<<<1, 1, 0, s>>>(d);
+  launches += scan_exclusive(d.candFlag, d.candMaskOff, d.capCand, d.candMaskOff + d.capCand, d.scanPartial, s);
+  k_excl<true><<<exGrid, 256, 0, s>>>(d);  // also maskCount
   // work items
-  scan_exclusive(d.workCountPerBlock, d.workOffset, d.maxBlocks, d.workOffset + d.maxBlocks,
+  launches += scan_exclusive(d.workCountPerBlock, d.workOffset, d.maxBlocks, d.workOffset + d.maxBlocks,
                  d.scanPartial, s);
   k_work<<<grid_for(d.maxBlocks, 256), 256, 0, s>>>(d);
   return launches;

@@ -6,7 +6,8 @@
 
 namespace bnb {
 // Exclusive scan of n ints into out[0..n); the total goes to *total.
-void scan_exclusive(const int *in, int *out, int n, int *total, int *partial, cudaStream_t s);
+// Returns the number of kernels launched (1 up to 16,384 items, else 3).
+int scan_exclusive(const int *in, int *out, int n, int *total, int *partial, cudaStream_t s);
 // Full list rebuild (bin, sort, blocks, AABBs, cull at sqrt(rcull2), masks, work items).
 // Returns the number of kernels launched.
 int rebuild_list(const Dev &d, const int *colRep, const float *pos, float rcull2, cudaStream_t s);
