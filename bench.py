@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref", action="store_true", help="skip the reference CUDA comparison leg")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--ref-seconds", type=float, default=60.0,
+                    help="reference arm: CPU seconds for warm-up plus timed steps")
     return ap.parse_args()
 
 
@@ -150,7 +152,7 @@ def run_reference(args, rank, world):
     full = sampler.run(x, 0, s.N)
     t_full = time.perf_counter() - t0
     # window per step so that warm-up + timed steps take about a minute
-    budget = 60.0
+    budget = args.ref_seconds
     frac = min(1.0, budget / max(1e-9, (args.steps + args.warmup) * t_full))
     win = max(32, int(s.N * frac))
     rng = np.random.default_rng(7)
@@ -175,6 +177,20 @@ def run_reference(args, rank, world):
                              "sample": sample},
             "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def aggregate_over_ranks(t_total, t_e2e, pairs, world, device):
+    """Whole-job numbers: the slowest rank's device times, the pairs of all
+    ranks (every rank processes its own replica, so work adds up)."""
+    if world <= 1:
+        return t_total, t_e2e, pairs
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([t_total, t_e2e if t_e2e is not None else 0.0], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    p = torch.tensor([pairs], dtype=torch.float64, device=device)
+    dist.all_reduce(p, op=dist.ReduceOp.SUM)
+    return float(t[0]), (float(t[1]) if t_e2e is not None else None), float(p[0])
 
 
 # ---------------------------------------------------------------------------
@@ -312,16 +328,7 @@ def run_bnb(args, rank, world):
         else:
             ref_cuda = {"unavailable": "oracle/_ref/libbladeref.so not built"}
 
-    # aggregate over ranks: max time, summed pairs
-    if world > 1:
-        t = torch.tensor([t_total, e2e["t"] if e2e else 0.0], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        p = torch.tensor([P], dtype=torch.float64, device=dev)
-        dist.all_reduce(p, op=dist.ReduceOp.SUM)
-        t_total, t_e2e_max, P_all = float(t[0]), float(t[1]), float(p[0])
-    else:
-        P_all = P
-        t_e2e_max = e2e["t"] if e2e else None
+    t_total, t_e2e_max, P_all = aggregate_over_ranks(t_total, e2e["t"] if e2e else None, P, world, dev)
 
     if rank != 0:
         return
