@@ -92,3 +92,51 @@ def test_no_fallback_when_library_missing(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "_lib", None)
     with pytest.raises(RuntimeError):
         _lib.lib()
+
+
+def test_pme_call_order_and_arguments():
+    lib = _lib.lib()
+    p = _lib.Params()
+    lib.bnb_default_params(C.byref(p))
+    h = C.c_void_p()
+    counts = np.array([0], np.int32)
+    assert lib.bnb_create(C.byref(p), 1, counts.ctypes.data_as(C.c_void_p), C.byref(h)) == 0
+    box = np.full(3, 40.0, np.float32)
+    bp = box.ctypes.data_as(C.c_void_p)
+    out = _lib.Outputs()
+    K = np.zeros(3, np.int32)
+    for order in (0, 3, 5, 10):                      # orders 4, 6, 8 only (nbrecip.cu:537-545)
+        assert lib.bnb_set_pme(h, order, C.c_float(1.0), None, bp) == _lib.BNB_ERR_ARG
+    assert lib.bnb_set_pme(h, 6, C.c_float(0.0), None, bp) == _lib.BNB_ERR_ARG   # no spacing, no grid
+    assert lib.bnb_set_pme(h, 6, C.c_float(1.0), None, None) == _lib.BNB_ERR_ARG
+    assert lib.bnb_set_pme(h, 6, C.c_float(1.0), None, bp) == _lib.BNB_ERR_STATE  # before the topology
+    assert lib.bnb_pme_grid(h, 0, K.ctypes.data_as(C.c_void_p)) == _lib.BNB_ERR_STATE
+    assert lib.bnb_compute_pme(h, None, None, bp, 1, C.byref(out), None) == _lib.BNB_ERR_STATE
+    assert lib.bnb_compute_ewald_self(h, None, 1, C.byref(out), None) == _lib.BNB_ERR_STATE
+    assert lib.bnb_compute_pme(h, None, None, None, 1, C.byref(out), None) == _lib.BNB_ERR_ARG
+    lib.bnb_destroy(h)
+
+
+def test_constraint_and_split_step_arguments():
+    lib = _lib.lib()
+    x = np.zeros(9)
+    xp = x.ctypes.data_as(C.c_void_p)
+    empty = _lib.ConstraintSet(0, 0, 0, 0, None, None, None, None)
+    assert lib.bnb_holonomic_position(None, xp, xp, None, xp, 0.02, 1e-10, 10, None, None, None) == _lib.BNB_ERR_ARG
+    bad = _lib.ConstraintSet(-1, 0, 0, 0, None, None, None, None)
+    assert lib.bnb_holonomic_position(C.byref(bad), xp, xp, None, xp, 0.02, 1e-10, 10, None, None,
+                                      None) == _lib.BNB_ERR_ARG
+    missing = _lib.ConstraintSet(2, 0, 0, 0, None, None, None, None)   # a count without its array
+    assert lib.bnb_holonomic_velocity(C.byref(missing), xp, xp, xp, None) == _lib.BNB_ERR_ARG
+    for halfdt, tol, it in ((0.0, 1e-10, 10), (0.02, 0.0, 10), (0.02, 1e-10, 0)):
+        assert lib.bnb_holonomic_position(C.byref(empty), xp, xp, None, xp, halfdt, tol, it, None, None,
+                                          None) == _lib.BNB_ERR_ARG
+    # nothing to constrain: success without a launch
+    assert lib.bnb_holonomic_position(C.byref(empty), xp, xp, None, xp, 0.02, 1e-10, 10, None, None, None) == 0
+    assert lib.bnb_holonomic_velocity(C.byref(empty), xp, xp, xp, None) == 0
+    args = (xp, xp, xp, xp, xp, xp, xp, xp, xp, 0.04, 0.9, 0.3, 0.9, 0.3, C.c_ulonglong(1), C.c_ulonglong(0),
+            None, None, None, None)
+    assert lib.bnb_langevin_half(2, 3, 0, *args) == _lib.BNB_ERR_ARG
+    assert lib.bnb_langevin_half(0, 0, 0, *args) == 0
+    assert lib.bnb_langevin_half(0, 3, 0, xp, xp, None, None, xp, None, None, None, None, 0.04, 0.9, 0.3, 0.9,
+                                 0.3, C.c_ulonglong(1), C.c_ulonglong(0), None, None, None, None) == _lib.BNB_ERR_ARG

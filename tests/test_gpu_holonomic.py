@@ -117,3 +117,20 @@ def test_batch_with_rigid_waters(cuda):
     d12 = np.linalg.norm(x[tri["idx"][:, 1]] - x[tri["idx"][:, 2]], axis=1)
     assert np.abs(d01 - 0.9572).max() < 1e-6 and np.abs(d12 - 1.5139).max() < 1e-6
     B.close()
+
+
+def test_empty_and_single_cluster_types(cuda):
+    """Each cluster type alone, and an empty set (no launch)."""
+    T, B1, B2, B3, xp, x, ism = H.test_clusters(seed=8, n_water=3, n_each=2, jitter=0.02)
+    for sets in ((T, None, None, None), (None, B1, None, None), (None, None, B2, None), (None, None, None, B3)):
+        cs = Constraints(*sets)
+        xg = _t(x)
+        cs.position(_t(xp), xg, None, _t(ism), 0.02, tolerance=1e-12, max_iter=20)
+        args = [a if a is not None else np.zeros(0, d) for a, d in
+                zip(sets, (H.TRI_DTYPE, H.B1_DTYPE, H.B2_DTYPE, H.B3_DTYPE))]
+        xo, _, _ = H.constrain_position(H.clusters(*args), xp, x, ism, 0.02)
+        assert np.abs(xg.cpu().numpy().reshape(-1, 3) - xo).max() < 1e-10
+    cs = Constraints()
+    xg = _t(x)
+    cs.position(_t(xp), xg, None, _t(ism), 0.02)
+    assert np.array_equal(xg.cpu().numpy(), np.ascontiguousarray(x, np.float64).reshape(-1))

@@ -160,3 +160,26 @@ def test_recip_matches_reference_golden(cuda, path):
         assert _rel(l.cpu().numpy()[1:], z["lambdaForce"][1:]) < REF_FORCE_TOL
         assert _rel(ls.cpu().numpy()[1:], z["self_lambdaForce"][1:]) < 1e-5
     nb.close()
+
+
+def test_zero_charges_and_non_pme_methods(cuda):
+    s = systems.water_box()
+    s.nbonds["q"] = 0
+    nb = NbDirect(s)
+    nb.set_pme(order=6)
+    f, _, e = nb.evaluate_pme()
+    assert float(f.abs().max().cpu()) == 0.0 and float(e.cpu()[0]) == 0.0
+    ls, es = nb.evaluate_ewald_self()
+    assert float(es.cpu()[0]) == 0.0
+    nb.close()
+    s2 = systems.water_box()
+    s2.elecMethod = 0                                # FSWITCH: no reciprocal space (nbrecip.cu:486)
+    nb = NbDirect(s2)
+    nb.set_pme(order=6)
+    e64 = torch.full((1,), 5.0, dtype=torch.float64, device="cuda")
+    f64 = torch.full((3 * s2.N,), 7.0, dtype=torch.float64, device="cuda")
+    nb.getforce_ewald(nb.positions_tensor(), None, True, force64=f64, energy64=e64)
+    nb.getforce_ewaldself(None, True, energy64=e64)
+    torch.cuda.synchronize()
+    assert float(e64.cpu()[0]) == 5.0 and bool((f64 == 7.0).all())
+    nb.close()
