@@ -183,3 +183,32 @@ def test_zero_charges_and_non_pme_methods(cuda):
     torch.cuda.synchronize()
     assert float(e64.cpu()[0]) == 5.0 and bool((f64 == 7.0).all())
     nb.close()
+
+
+def test_capture_in_cuda_graph(cuda):
+    """The reciprocal evaluation (cuFFT plans made beforehand) records into a
+    CUDA graph; replays give the eager bits."""
+    s = systems.water_box()
+    nb = NbDirect(s)
+    nb.set_pme(order=6)
+    pos = nb.positions_tensor()
+    f_eager, _, e_eager = nb.evaluate_pme(pos)
+    f64 = torch.zeros(3 * s.N, dtype=torch.float64, device="cuda")
+    e64 = torch.zeros(1, dtype=torch.float64, device="cuda")
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):                       # warm-up outside capture
+        nb.getforce_ewald(pos, None, True, force64=f64, energy64=e64)
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        nb.getforce_ewald(pos, None, True, force64=f64, energy64=e64)
+    f64.zero_()
+    e64.zero_()
+    g.replay()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(f64.reshape(-1, 3), f_eager) and torch.equal(e64, e_eager)
+    del g
+    nb.close()
