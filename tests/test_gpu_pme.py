@@ -212,3 +212,33 @@ def test_capture_in_cuda_graph(cuda):
     assert torch.equal(f64.reshape(-1, 3), f_eager) and torch.equal(e64, e_eager)
     del g
     nb.close()
+
+
+def test_total_electrostatics_matches_oracle_and_is_beta_invariant(cuda):
+    """The four electrostatic pieces on the GPU -- bnb_compute (direct),
+    bnb_compute_nbex, bnb_compute_pme, bnb_compute_ewald_self -- add up to
+    the oracle's Ewald total, and the total does not depend on beta."""
+    import dataclasses as dc
+    import oracle
+    base = systems.with_pair_lists(systems.water_box())
+    q = base.nbonds["q"].astype(np.float64)
+    totals = []
+    for beta in (0.34, 0.40):
+        s = dc.replace(base, betaEwald=beta)
+        nb = NbDirect(s)
+        pos = nb.positions_tensor()
+        nb.update_domdec(pos, True)
+        ed = float(nb.evaluate(pos)[2][0])
+        nb.set_pairs()
+        ex = float(nb.evaluate_pairs("nbex", pos)[2][0])
+        nb.set_pme(order=8, grid=(40, 40, 40))
+        er = float(nb.evaluate_pme(pos)[2][0])
+        es = float(nb.evaluate_ewald_self()[1][0])
+        nb.close()
+        parts = (oracle.nbdirect(s)["energy"], oracle.pair_lists(s, which="nbex")["energy"],
+                 pme_oracle.pme_recip(s.xyz, q, s.box, [40, 40, 40], 8, beta, K_ELECTRIC)[0],
+                 pme_oracle.ewald_self(q, beta, K_ELECTRIC)[0])
+        scale = max(abs(p) for p in parts)
+        assert abs((ed + ex + er + es) - sum(parts)) < 2e-6 * scale
+        totals.append(ed + ex + er + es)
+    assert abs(totals[0] - totals[1]) < 2e-5 * scale

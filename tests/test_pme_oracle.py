@@ -91,3 +91,24 @@ def test_translation_invariance():
     E2, g2, _, _ = P.pme_recip(s.xyz.astype(np.float64) + shift, q, s.box, K, 6, 0.34, K_ELECTRIC)
     assert E2 == pytest.approx(E, rel=1e-10)
     assert np.allclose(g2, g, atol=1e-8)
+
+
+def test_total_electrostatics_is_beta_invariant():
+    """Direct space (erfc, cutoff) + nbex exclusion corrections + PME
+    reciprocal + self term is the Ewald sum, whose value does not depend on
+    the splitting parameter beta: beta 0.34 and 0.40 agree to the direct-space
+    truncation erfc(beta rCut) (1.2e-5 at beta 0.34, rCut 9 A) of the
+    components' scale."""
+    import dataclasses as dc
+    import oracle
+    base = systems.with_pair_lists(systems.water_box())
+    q = base.nbonds["q"].astype(np.float64)
+    totals, scale = [], 0.0
+    for beta in (0.34, 0.40):
+        s = dc.replace(base, betaEwald=beta)
+        parts = (oracle.nbdirect(s)["energy"], oracle.pair_lists(s, which="nbex")["energy"],
+                 P.pme_recip(s.xyz, q, s.box, [40, 40, 40], 8, beta, K_ELECTRIC)[0],
+                 P.ewald_self(q, beta, K_ELECTRIC)[0])
+        totals.append(sum(parts))
+        scale = max(scale, max(abs(p) for p in parts))
+    assert abs(totals[0] - totals[1]) < 2e-5 * scale
