@@ -15,7 +15,11 @@ rigid instead (holonomic triangles, src/holonomic/holonomic.cu): the update
 is split at its middle (bnb_langevin_half) and bnb_holonomic_position follows
 each half drift, as update_VVhbpR / holonomic_position / update_OOhbpR /
 holonomic_position do (update.cu:276-303), with true hydrogen masses and
-the water bonds dropped.  All replicas share one libbnb handle, so every kernel of a step
+the water bonds dropped.  With ``pme=True`` the electrostatics are complete:
+the 1-4 pairs and exclusion corrections (bnb_compute_nb14 / bnb_compute_nbex,
+lists from systems.with_pair_lists), PME reciprocal space and the Ewald self
+term (bnb_compute_pme / bnb_compute_ewald_self), as Potential::calc_force
+sums them (src/system/potential.cxx:1851-1941).  All replicas share one libbnb handle, so every kernel of a step
 covers all of them; ``capture`` records ``rebuild_every`` steps in one CUDA
 graph that is replayed.  Units are AKMA; dt is 2 fs.
 """
@@ -67,9 +71,12 @@ class MsldBatch:
 
     def __init__(self, reps: list[System], dt_fs: float = 2.0, T: float = 300.0, gamma_ps: float = 1.0,
                  seed: int = 1, rebuild_every: int = 10, energy_every: int = 10, device="cuda", tune=False,
-                 theta_mass: float = THETA_MASS, gamma_theta_ps: float | None = None, constraints: bool = False):
+                 theta_mass: float = THETA_MASS, gamma_theta_ps: float | None = None, constraints: bool = False,
+                 pme: bool = False, pme_order: int = 6):
         import torch
         self.torch = torch
+        if pme:                                            # 1-4 pairs join the exclusions; nbex lists
+            reps = [systems.with_pair_lists(s) for s in reps]
         self.reps = reps
         self.dev = torch.device(device)
         self.nb = NbDirect(reps, device=self.dev)
@@ -166,6 +173,13 @@ class MsldBatch:
         self.fixed_bias = None                             # lambda biases (set_bias)
         self.var_bias = None
         self.hist1 = None                                  # lambda histograms (enable_histograms)
+        self.pme = pme
+        if pme:
+            self.nb.set_pairs()
+            self.nb.set_pme(order=pme_order)
+            self.f_term = torch.zeros(3 * N, dtype=f64, device=self.dev)   # per-term outputs, then added
+            self.l_term = torch.zeros(L, dtype=f64, device=self.dev)
+            self.e_term = torch.zeros(self.nb.R, dtype=f64, device=self.dev)
         self.nb.update_domdec(self.xf, True)               # synchronous first build sizes the list
         if tune:
             self.tuned_ms = self.autotune()
@@ -190,6 +204,22 @@ class MsldBatch:
         if self.bond_start is not None:
             _lib.call("bnb_bond_gradient", self.nb.N, _p(self.bond_start), _p(self.bond_partner),
                       _p(self.bond_param), _p(self.x), _p(self.force), s)
+        if self.pme:                                       # the other electrostatic terms of calc_force
+            for term in ("nb14", "nbex", "recip", "self"):
+                e = self.e_term if calc_e else None
+                if term == "recip":
+                    nb.getforce_ewald(self.xf, self.lamf, calc_e, force64=self.f_term, lambda_force64=self.l_term,
+                                      energy64=e, stream=stream)
+                elif term == "self":
+                    nb.getforce_ewaldself(self.lamf, calc_e, lambda_force64=self.l_term, energy64=e, stream=stream)
+                else:
+                    nb.getforce_pairs(term, self.xf, self.lamf, calc_e, force64=self.f_term,
+                                      lambda_force64=self.l_term, energy64=e, stream=stream)
+                if term != "self":
+                    self.force.add_(self.f_term)
+                self.lforce.add_(self.l_term)
+                if calc_e:
+                    self.energy.add_(self.e_term)
         if self.fixed_bias is not None:
             _lib.call("bnb_bias", self.theta.numel(), _p(self.lam), _p(self.fixed_bias), self.n_var,
                       _p(self.var_bias), _p(self.lforce), None, s)

@@ -59,7 +59,7 @@ def run_batch(args):
     atoms = [r.N for r in reps]
     K = args.steps
     # batched: one handle, autotuned, one CUDA graph per 10 steps
-    B = MsldBatch(reps, tune=True, constraints=args.constraints)
+    B = MsldBatch(reps, tune=True, constraints=args.constraints, pme=args.pme)
     tuning = B.tuning()
     B.capture()
     B.run_graph(20)
@@ -95,7 +95,7 @@ def run_batch(args):
     t_seq_graph = 0.0
     bad = 0
     for r in reps:
-        S = MsldBatch([r], tune=args.tune_sequential, constraints=args.constraints)
+        S = MsldBatch([r], tune=args.tune_sequential, constraints=args.constraints, pme=args.pme)
         S.run_eager(10)
         torch.cuda.synchronize()
         a, b = _events()
@@ -121,7 +121,9 @@ def run_batch(args):
             "steps": K, "step": ("rebuild/10 + nbdirect(MSLD) + dU/dlambda->dU/dtheta + Langevin VRORV(x, theta) "
                                  + ("split around holonomic constraints (rigid TIP3P, true H masses) + chain bonds"
                                     if args.constraints else "+ harmonic bonds (HMR)")
-                                 + " + theta->lambda; no PME recip, angles or dihedrals"),
+                                 + (" + nb14 + nbex + PME reciprocal + Ewald self" if args.pme else "")
+                                 + " + theta->lambda; no angles or dihedrals"
+                                 + ("" if args.pme else ", no PME reciprocal")),
             "batched_graph": {"seconds": t_batch, "ns_per_day_aggregate": ns_per_day(K, t_batch, replicas=R),
                               "tuning": tuning, "status": st, "nan": nan, "breakdown": breakdown},
             "sequential_eager": {"seconds": t_seq, "ns_per_day_aggregate": ns_per_day(K, t_seq, replicas=R)},
@@ -273,6 +275,7 @@ def main(argv=None):
     ap.add_argument("--eval-modes", default="plain,learned:1")
     ap.add_argument("--target", default="flat", choices=["flat", "lookahead"])
     ap.add_argument("--constraints", action="store_true", help="batch: rigid waters (holonomic constraints)")
+    ap.add_argument("--pme", action="store_true", help="batch: 1-4, exclusion corrections, PME reciprocal, self")
     args, rest = ap.parse_known_args(argv)
     if args.what == "batch":
         run_batch(args)
