@@ -27,10 +27,10 @@ extern "C" {
 #define BNB_ERR_ARG 1          /* bad argument (null, size, method)          */
 #define BNB_ERR_CUDA 2         /* a CUDA call failed                         */
 #define BNB_ERR_CAPACITY 3     /* list capacity exceeded and could not grow  */
-#define BNB_ERR_UNSUPPORTED 4  /* feature outside this build (see message)   */
+#define BNB_ERR_UNSUPPORTED 4  /* feature this library does not implement     */
 #define BNB_ERR_STATE 5        /* call order (e.g. compute before rebuild)   */
 #define BNB_ERR_DEVICE 6       /* device status word reports a failure       */
-#define BNB_ERR_TOO_LARGE 7    /* size above a fixed limit of this build     */
+#define BNB_ERR_TOO_LARGE 7    /* size above a fixed limit of this library   */
 
 /* ---- device status bits (bnb_status) ------------------------------------ */
 #define BNB_STATUS_BLOCK_OVERFLOW 1
