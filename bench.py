@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref", action="store_true", help="skip the reference CUDA comparison leg")
+    ap.add_argument("--no-pme", action="store_true", help="skip the PME reciprocal-space leg")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-seconds", type=float, default=60.0,
                     help="reference arm: CPU seconds for warm-up plus timed steps")
@@ -323,6 +324,37 @@ def run_bnb(args, rank, world):
         else:
             ref_cuda = {"unavailable": "oracle/_ref/libbladeref.so not built"}
 
+    # the next row, PME reciprocal space on the same system (order 6, 1 A grid):
+    # device time per evaluation, energy every 10th, next to the reference's
+    # getforce_ewald on the same GPU (outside the headline's timed region)
+    pme = None
+    if world == 1 and not args.no_pme:
+        nb.set_pme(order=6, grid_space=1.0)
+        pos0 = frames[W]
+        fp = torch.zeros(3 * s.N, dtype=torch.float32, device=dev)
+        ep = torch.zeros(1, dtype=torch.float64, device=dev)
+        reps = 200
+        for k in range(10):
+            nb.getforce_ewald(pos0, None, k % ENERGY_EVERY == 0, force=fp, energy=ep)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for k in range(reps):
+            nb.getforce_ewald(pos0, None, k % ENERGY_EVERY == 0, force=fp, energy=ep)
+        b.record(stream)
+        torch.cuda.synchronize()
+        pme = {"grid": list(nb.pme_grid(0)), "order": 6, "ms_per_eval": a.elapsed_time(b) / reps}
+        if not args.no_ref:
+            from oracle import refgpu
+            if refgpu.available():
+                try:
+                    rp = refgpu.RefGPU(s)
+                    rp.set_state(frames[W].double().cpu().numpy().reshape(-1, 3))
+                    rp.set_pme(6, pme["grid"])
+                    rp.time_pme(10, ENERGY_EVERY)
+                    pme["reference_ms_per_eval"] = rp.time_pme(reps, ENERGY_EVERY) / reps
+                except Exception as exc:  # report, do not hide
+                    pme["reference"] = {"unavailable": str(exc)}
+
     t_total, t_e2e_max, P_all = aggregate_over_ranks(t_total, e2e["t"] if e2e else None, P, world, dev)
 
     if rank != 0:
@@ -353,6 +385,8 @@ def run_bnb(args, rank, world):
     }
     if ref_cuda is not None:
         line["reference_cuda_same_gpu"] = ref_cuda
+    if pme is not None:
+        line["pme_reciprocal"] = pme
     if e2e:
         line["e2e"] = {"value": P_all / t_e2e_max, "unit": "pairs/s", "h2d_bytes_per_step": e2e["h2d"],
                        "d2h_bytes_per_step": e2e["d2h"]}
