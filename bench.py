@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref", action="store_true", help="skip the reference CUDA comparison leg")
     ap.add_argument("--no-pme", action="store_true", help="skip the PME reciprocal-space leg")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default tuning (no autotuner)")
+    ap.add_argument("--tuning", default=None, help="T,C: fixed tiles per work item and CTAs per SM")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-seconds", type=float, default=60.0,
                     help="reference arm: CPU seconds for warm-up plus timed steps")
@@ -228,9 +230,21 @@ def run_bnb(args, rank, world):
         calc_e = all_energy or k % ENERGY_EVERY == 0
         nb.getforce_nbdirect(pos, None, calc_e, force=force, energy=energy)
 
-    # warm-up (first rebuild is synchronous and sizes the list)
+    # warm-up (first rebuild is synchronous and sizes the list), then the
+    # autotuner picks tiles per work item x CTAs per SM on this system
     for k in range(W):
         step(k, frames[k])
+    tuning = None
+    if args.tuning:
+        t, c = (int(v) for v in args.tuning.split(","))
+        nb.set_tuning(t, c)
+        for k in range(W):
+            step(k, frames[k])
+        tuning = {"tiles_per_work": t, "ctas_per_sm": c, "source": "--tuning"}
+    elif not args.no_tune:
+        tuning = nb.autotune(frames[0])
+        for k in range(W):
+            step(k, frames[k])
     torch.cuda.synchronize()
     st = nb.status(clear=True)
     if st:
@@ -372,7 +386,8 @@ def run_bnb(args, rank, world):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded chain-in-water, 23,558 atoms per GPU)",
         "config": {"workload": WORKLOAD, "atoms": s.N, "pairs_per_step": P / K, "jitter_A": JITTER,
                    "energy_every": ENERGY_EVERY,
-                   "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}"},
+                   "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}",
+                   "tuning": tuning},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_t, "unit": "TFLOP/s",
                      "frac": achieved / peak_t, "traffic": traffic,
                      "kernel": "k_pair<PME,VFSWITCH> (per-launch mean over the timed region)",

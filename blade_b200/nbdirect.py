@@ -208,6 +208,23 @@ class NbDirect:
         self.getforce_ewaldself(lam, True, lambda_force64=l64, energy64=e64)
         return l64, e64
 
+    # -- tuning -------------------------------------------------------------------
+    def set_tuning(self, tiles_per_work: int, ctas_per_sm: int = 0):
+        """bnb_set_tuning: candidate tiles per work item (4..32) and resident CTAs
+        per SM of the persistent pair kernel (0 = occupancy); the next rebuild applies it."""
+        _lib.call("bnb_set_tuning", self.h, int(tiles_per_work), int(ctas_per_sm))
+
+    def autotune(self, positions, lambdas=None, reps: int = 5, stream=None) -> dict:
+        """bnb_autotune: tries tiles per work item x CTAs per SM on this system,
+        keeps the fastest (median of ``reps``), rebuilds the list; returns the choice."""
+        best = C.c_float()
+        b = np.ascontiguousarray(self.boxes, np.float32)
+        _lib.call("bnb_autotune", self.h, _ptr(positions), _ptr(lambdas), b.ctypes.data_as(C.c_void_p), int(reps),
+                  _stream(stream), C.byref(best))
+        t, c = C.c_int(), C.c_int()
+        _lib.call("bnb_get_tuning", self.h, C.byref(t), C.byref(c))
+        return {"tiles_per_work": t.value, "ctas_per_sm": c.value, "best_ms": best.value}
+
     # -- conveniences ------------------------------------------------------------
     def positions_tensor(self, xyz_list=None):
         import torch

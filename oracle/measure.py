@@ -42,6 +42,7 @@ def run_msld(args, water_only=False):
     pos = nb.positions_tensor()
     lam = nb.lambdas_tensor()
     nb.update_domdec(pos, True)
+    tuning = nb.autotune(pos, lam)
     nb.set_counting(True)
     f64, l64, e64 = nb.evaluate(pos, lam)
     pairs = nb.pair_count()
@@ -71,7 +72,7 @@ def run_msld(args, water_only=False):
                        "msld_water (216-water box + 3 sites x 4 substituents, soft core)"), "atoms": s.N,
             "lambda_blocks": s.msld.blockCount if s.msld else 1, "pairs_per_eval": pairs, "pairs_oracle": o["pairs"],
             "force_rel_rms_vs_fp64": ferr, "dUdlambda_rel_rms_vs_fp64": lerr, "energy_rel_err_vs_fp64": e_rel,
-            "bnb": {"pairs_per_s": pairs * K / t, "ms_per_step": 1e3 * t / K}}
+            "bnb": {"pairs_per_s": pairs * K / t, "ms_per_step": 1e3 * t / K, "tuning": tuning}}
     if refgpu.available():
         ref = refgpu.RefGPU(s)
         r = ref.evaluate()
