@@ -58,7 +58,7 @@ struct Counters {
 struct Dev {
   // --- static topology (set_topology) -------------------------------------
   int N, R, nTypes, ljCombine, lamTotal;
-  int tilesPerWork;        // candidate tiles per work item (tuning knob, 4..32)
+  int tilesPerWork;        // candidate tiles per work item (tuning knob, 2..32)
   RepInfo *rep;            // [R]
   int *atomRep;            // [N]
   float *atomQ;            // [N] charge * sqrt(kElectric)
