@@ -81,6 +81,7 @@ struct bnb_handle {
   float *pmeMod_d = nullptr, *pmeGrid_d = nullptr;
   float2 *pmeCplx_d = nullptr;
   long long *pmeFix_d = nullptr, *pmeAccL = nullptr, *pmeAccE = nullptr;
+  unsigned int *pmeDone = nullptr;
 };
 
 namespace {
@@ -1148,6 +1149,7 @@ bnb::PmeArgs pme_args(bnb_handle *h, const float *position, const float *lambda)
   a.cplx = h->pmeCplx_d;
   a.accL = h->pmeAccL;
   a.accE = h->pmeAccE;
+  a.done = h->pmeDone;
   return a;
 }
 }  // namespace
@@ -1185,7 +1187,7 @@ extern "C" int bnb_set_pme(bnb_handle *h, int order, float gridSpace, const int 
   Arena a;
   size_t oRep = a.take<bnb::PmeRep>(std::max(R, 1)), oMod = a.take<float>(mOff), oFix = a.take<long long>(gOff),
          oGrid = a.take<float>(gOff), oCplx = a.take<float2>(cOff), oL = a.take<long long>(std::max(h->lamTotal, 1)),
-         oE = a.take<long long>(std::max(R, 1));
+         oE = a.take<long long>(std::max(R, 1)), oDone = a.take<unsigned int>(1);
   void *base = nullptr;
   if (!ok(cudaMalloc(&base, a.off))) return BNB_ERR_CUDA;
   h->pmeArena = base;
@@ -1197,6 +1199,7 @@ extern "C" int bnb_set_pme(bnb_handle *h, int order, float gridSpace, const int 
   h->pmeCplx_d = (float2 *)(b + oCplx);
   h->pmeAccL = (long long *)(b + oL);
   h->pmeAccE = (long long *)(b + oE);
+  h->pmeDone = (unsigned int *)(b + oDone);
   std::vector<float> mod(mOff);
   for (int r = 0; r < R; r++) {
     float *m = mod.data() + pr[r].modOff;
@@ -1277,7 +1280,7 @@ extern "C" int bnb_compute_pme(bnb_handle *h, const float *position, const float
             CUFFT_SUCCESS)
       return BNB_ERR_CUDA;
   }
-  h->launches += 5;
+  h->launches += 4;
   return bnb::pme_gather(a, *out, calcEnergy != 0, s);
 }
 
@@ -1288,6 +1291,6 @@ extern "C" int bnb_compute_ewald_self(bnb_handle *h, const float *lambda, int ca
   if (h->alch && !lambda) return BNB_ERR_ARG;
   if (h->p.elecMethod != 1) return BNB_OK;  // nbrecip.cu:64
   bnb::PmeArgs a = pme_args(h, nullptr, lambda);
-  h->launches += 2;
+  h->launches += 1;
   return bnb::pme_self(a, *out, calcEnergy != 0, (cudaStream_t)stream);
 }

@@ -172,6 +172,41 @@ __global__ void k_convolve(PmeArgs a) {
   }
 }
 
+// lambda and energy accumulators -> outputs, by the calling CTA's threads.
+__device__ void finalize_outputs(const PmeArgs &a, const bnb_outputs &o, bool energy) {
+  const double inv = 1.0 / kFixScale;
+  for (int i = threadIdx.x; i < a.lamTotal; i += blockDim.x) {
+    const long long v = __ldcg(&a.accL[i]);
+    a.accL[i] = 0;
+    const double f = (double)v * inv;
+    if (o.lambdaForce64) o.lambdaForce64[i] = f;
+    if (o.lambdaForce && v) atomicAdd(&o.lambdaForce[i], (float)f);
+  }
+  if (energy)
+    for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
+      const long long v = __ldcg(&a.accE[r]);
+      a.accE[r] = 0;
+      const double e = (double)v * inv;
+      if (o.energy64) o.energy64[r] = e;
+      if (o.energy) o.energy[r] += e;
+    }
+}
+
+// The last CTA of a launch to finish writes the lambda and energy outputs
+// (every CTA's reductions are fenced before it takes its ticket), so no
+// separate finalize launch follows the gather.
+__device__ void finalize_if_last(const PmeArgs &a, const bnb_outputs &o, bool energy) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(a.done, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  finalize_outputs(a, o, energy);
+  if (threadIdx.x == 0) *a.done = 0;  // ready for the next launch
+}
+
 // ---------------------------------------------------------------------------
 // Gather: same lane layout as the spread; the 8 lanes of an atom reduce with
 // xor shuffles, lane 0 of the group writes the atom's outputs.
@@ -273,13 +308,14 @@ __global__ void __launch_bounds__(256) k_gather(PmeArgs a, bnb_outputs o) {
       red_add(&a.accE[r], ef);
     }
   }
+  finalize_if_last(a, o, ENERGY);
 }
 
 // ---------------------------------------------------------------------------
 // Ewald self term: one thread per atom.
 // ---------------------------------------------------------------------------
 template <bool ENERGY>
-__global__ void k_self(PmeArgs a, float pre) {
+__global__ void k_self(PmeArgs a, float pre, bnb_outputs o) {
   const int lane = threadIdx.x & 31;
   const int atom = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = atom < a.N;
@@ -306,27 +342,11 @@ __global__ void k_self(PmeArgs a, float pre) {
       red_add(&a.accE[r], ef);
     }
   }
+  finalize_if_last(a, o, ENERGY);
 }
 
-// lambda and energy accumulators -> outputs (one CTA).
-__global__ void k_pme_finalize(PmeArgs a, bnb_outputs o, bool energy) {
-  const double inv = 1.0 / kFixScale;
-  for (int i = threadIdx.x; i < a.lamTotal; i += blockDim.x) {
-    const long long v = a.accL[i];
-    a.accL[i] = 0;
-    const double f = (double)v * inv;
-    if (o.lambdaForce64) o.lambdaForce64[i] = f;
-    if (o.lambdaForce && v) atomicAdd(&o.lambdaForce[i], (float)f);
-  }
-  if (energy)
-    for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
-      const long long v = a.accE[r];
-      a.accE[r] = 0;
-      const double e = (double)v * inv;
-      if (o.energy64) o.energy64[r] = e;
-      if (o.energy) o.energy[r] += e;
-    }
-}
+// lambda and energy accumulators -> outputs when there are no atoms (one CTA).
+__global__ void k_pme_finalize(PmeArgs a, bnb_outputs o, bool energy) { finalize_outputs(a, o, energy); }
 
 inline int grid_of(long long threads, int block) {
   long long g = (threads + block - 1) / block;
@@ -368,8 +388,9 @@ int pme_gather(const PmeArgs &a, const bnb_outputs &o, bool energy, cudaStream_t
       case 17: k_gather<8, true><<<grid, 256, 0, s>>>(a, o); break;
       default: return BNB_ERR_ARG;
     }
+  } else {
+    k_pme_finalize<<<1, 256, 0, s>>>(a, o, energy);
   }
-  k_pme_finalize<<<1, 256, 0, s>>>(a, o, energy);
   return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
 }
 
@@ -378,10 +399,11 @@ int pme_self(const PmeArgs &a, const bnb_outputs &o, bool energy, cudaStream_t s
   const float pre = (float)(-(double)a.beta / sqrt(kPi));
   if (a.N > 0) {
     const int grid = (a.N + 255) / 256;
-    if (energy) k_self<true><<<grid, 256, 0, s>>>(a, pre);
-    else k_self<false><<<grid, 256, 0, s>>>(a, pre);
+    if (energy) k_self<true><<<grid, 256, 0, s>>>(a, pre, o);
+    else k_self<false><<<grid, 256, 0, s>>>(a, pre, o);
+  } else {
+    k_pme_finalize<<<1, 256, 0, s>>>(a, o, energy);
   }
-  k_pme_finalize<<<1, 256, 0, s>>>(a, o, energy);
   return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
 }
 

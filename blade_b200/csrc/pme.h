@@ -32,6 +32,7 @@ struct PmeArgs {
   float2 *cplx;            // [totalCplx] spectrum
   long long *accL;         // [lamTotal]
   long long *accE;         // [R]
+  unsigned int *done;      // CTAs finished in the current gather / self launch (zero between launches)
 };
 
 // Spread lambda-scaled charges into qfix and convert to the FP32 grid
@@ -39,10 +40,10 @@ struct PmeArgs {
 int pme_spread(const PmeArgs &a, cudaStream_t s);
 // Multiply the spectrum by the influence function; one launch.
 int pme_convolve(const PmeArgs &a, cudaStream_t s);
-// Gather forces, dU/dlambda and energy from the potential grid, then write
-// the lambda and energy outputs; two launches.
+// Gather forces, dU/dlambda and energy from the potential grid; the last
+// CTA writes the lambda and energy outputs; one launch.
 int pme_gather(const PmeArgs &a, const bnb_outputs &o, bool energy, cudaStream_t s);
-// Ewald self energy and its dU/dlambda; two launches.
+// Ewald self energy and its dU/dlambda; one launch.
 int pme_self(const PmeArgs &a, const bnb_outputs &o, bool energy, cudaStream_t s);
 
 }  // namespace bnb
