@@ -126,6 +126,8 @@ def run_batch(args):
                                  + ("" if args.pme else ", no PME reciprocal")),
             "batched_graph": {"seconds": t_batch, "ns_per_day_aggregate": ns_per_day(K, t_batch, replicas=R),
                               "tuning": tuning, "status": st, "nan": nan, "breakdown": breakdown},
+            "sequential_tuning": ("autotuned per replica" if args.tune_sequential
+                                  else "default (--tune-sequential autotunes each replica: the fair baseline)"),
             "sequential_eager": {"seconds": t_seq, "ns_per_day_aggregate": ns_per_day(K, t_seq, replicas=R)},
             "sequential_graph": {"seconds": t_seq_graph,
                                  "ns_per_day_aggregate": ns_per_day(K, t_seq_graph, replicas=R)},
