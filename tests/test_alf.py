@@ -2,7 +2,6 @@
 layout against the reference's bias forms (through the oracle's FP64 bias
 routine), the update's fixed point on a synthetic landscape, and the
 relabeling tables used to augment the learned model's training data."""
-import math
 
 import numpy as np
 import pytest

@@ -3,7 +3,6 @@ step loop links it: the program compiles against include/bnb.h with gcc and
 links libbnb.so and the CUDA runtime, with no Python in the call path.  On the
 CPU it checks arguments and call order; on the GPU it evaluates the 216-water
 box and must give the bits of the Python host mirror."""
-import ctypes as C
 import os
 import subprocess
 

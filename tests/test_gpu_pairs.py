@@ -3,7 +3,6 @@ against the FP64 oracle: every method combination, MSLD scaling with and
 without the 1-4 soft core, two replicas on one handle, and repeated calls."""
 import numpy as np
 import pytest
-import torch
 
 import oracle
 from blade_b200 import systems
