@@ -231,7 +231,10 @@ int bnb_compute_nbex(bnb_handle *h, const float *position, const float *lambda,
  * bnb_compute's output semantics; energies are the eenbrecip term.
  * bnb_compute_ewald_self adds the self term (energy eenbrecipself and
  * dU/dlambda; no spatial force).  Both do nothing unless elecMethod is PME
- * (as the reference).  bnb_pme_grid returns the grid of one replica.
+ * (as the reference).  They share the handle's dU/dlambda and energy
+ * accumulators, so calls on one handle must be ordered (one stream, as the
+ * reference's nbrecipStream), not concurrent.  bnb_pme_grid returns the grid
+ * of one replica.
  */
 int bnb_set_pme(bnb_handle *h, int order, float gridSpace, const int *grid, const float *boxes);
 int bnb_pme_grid(bnb_handle *h, int replica, int *K);
