@@ -333,7 +333,7 @@ __device__ __forceinline__ void plain_loop(JRegs<COMBINE, ALCH> &J, const float4
 // with xor shuffles and returned to the owner lanes.
 // ---------------------------------------------------------------------------
 template <int ELEC, int VDW, int ALCH, bool ENERGY, bool COMBINE>
-__global__ void __launch_bounds__(256, ALCH ? 3 : 4) k_pair(KArgs A) {
+__global__ void __launch_bounds__(256, (ALCH || ENERGY) ? 3 : 4) k_pair(KArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int sIdx[8][32];
   const Dev &d = A.d;
