@@ -127,16 +127,21 @@ class ClockSampler:
                 "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
-def ncu_traffic_per_launch():
-    """DRAM bytes per pair-kernel launch from the committed ncu summary, if any."""
+def ncu_profile_value(key):
+    """A figure of the committed ncu summary of the pair kernel (``key: value``), if any."""
     path = os.path.join(ROOT, "profiles", "pair_kernel_chain_water_23558.md")
     try:
         for line in open(path):
-            if line.strip().startswith("traffic_bytes_per_launch:"):
+            if line.strip().startswith(key + ":"):
                 return float(line.split(":")[1].strip().split()[0])
     except OSError:
         pass
     return None
+
+
+def ncu_traffic_per_launch():
+    """DRAM bytes per pair-kernel launch from the committed ncu summary, if any."""
+    return ncu_profile_value("traffic_bytes_per_launch")
 
 
 # ---------------------------------------------------------------------------
@@ -391,6 +396,7 @@ def run_bnb(args, rank, world):
                      "frac": achieved / peak_t, "traffic": traffic,
                      "kernel": "k_pair<PME,VFSWITCH> (per-launch mean over the timed region)",
                      "flops_per_pair": FLOPS_PER_PAIR, "peak_source": "measured FP32 FMA chains (bnb_fp32_peak)",
+                     "mufu_pipe_pct_ncu": ncu_profile_value("mufu_pipe_pct"),
                      "pair_kernel_ms_mean": prof["pair_ms"] / max(1, prof["pair_launches"])},
         "rebuild_ms_mean": prof["rebuild_ms"] / max(1, prof["rebuilds"]),
         "ns_per_day_nbdirect_only": (K / t_total) * DT_FS * 86400 / 1e6,
