@@ -16,7 +16,7 @@ namespace bnb {
 constexpr int kNumShifts = 14;        // own image + 13 half-shell images
 constexpr int kExclBlk = 16;          // exclusion-partner blocks listed per block
 constexpr int kTilesPerWork = 8;      // default candidate tiles per pair-kernel work item
-constexpr int kMinTilesPerWork = 2;   // smallest setting (sizes the work-item capacity)
+constexpr int kMinTilesPerWork = 1;   // smallest setting (sizes the work-item capacity)
 constexpr int kMaxTableTypes = 64;    // LJ table kept in shared memory up to 64 types
 constexpr int kMaxLambdaShared = 2048;
 constexpr int kSortCap = 4096;        // column sort in shared memory up to 4096 atoms
@@ -58,7 +58,7 @@ struct Counters {
 struct Dev {
   // --- static topology (set_topology) -------------------------------------
   int N, R, nTypes, ljCombine, lamTotal;
-  int tilesPerWork;        // candidate tiles per work item (tuning knob, 2..32)
+  int tilesPerWork;        // candidate tiles per work item (tuning knob, 1..32)
   RepInfo *rep;            // [R]
   int *atomRep;            // [N]
   float *atomQ;            // [N] charge * sqrt(kElectric)

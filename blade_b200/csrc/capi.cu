@@ -757,7 +757,7 @@ int bnb_autotune(bnb_handle *h, const float *position, const float *lambda, cons
   if (!h || !boxes || (h->N > 0 && !position) || reps < 1) return BNB_ERR_ARG;
   if (!h->topo) return BNB_ERR_STATE;
   cudaStream_t s = (cudaStream_t)stream;
-  static const int kTiles[] = {2, 4, 8, 16, 32};
+  static const int kTiles[] = {1, 2, 4, 8, 16, 32};
   static const int kCtas[] = {0, 2, 3};
   bnb_outputs none;
   memset(&none, 0, sizeof(none));

@@ -210,7 +210,7 @@ class NbDirect:
 
     # -- tuning -------------------------------------------------------------------
     def set_tuning(self, tiles_per_work: int, ctas_per_sm: int = 0):
-        """bnb_set_tuning: candidate tiles per work item (2..32) and resident CTAs
+        """bnb_set_tuning: candidate tiles per work item (1..32) and resident CTAs
         per SM of the persistent pair kernel (0 = occupancy); the next rebuild applies it."""
         _lib.call("bnb_set_tuning", self.h, int(tiles_per_work), int(ctas_per_sm))
 

@@ -338,7 +338,7 @@ int bnb_bias_f32(int blockCount, const float *lambda, const float *fixedBias,
 
 /* ---- batched stepping: tuning and integrator ----------------------------- */
 /*
- * Tuning knobs of the pair kernel: candidate tiles per work item (2..32) and
+ * Tuning knobs of the pair kernel: candidate tiles per work item (1..32) and
  * CTAs per SM of the persistent grid (0 = as many as fit).  A changed tile
  * count takes effect at the next bnb_rebuild.  No reference counterpart.
  */

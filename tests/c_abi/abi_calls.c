@@ -43,7 +43,7 @@ static int argument_checks(void) {
   CHECK(bnb_compute(h, NULL, NULL, box, 1, &out, NULL), BNB_ERR_STATE);
   CHECK(bnb_set_pme(h, 5, 1.0f, NULL, box), BNB_ERR_ARG);           /* orders 4, 6, 8 */
   CHECK(bnb_set_pme(h, 6, 1.0f, NULL, box), BNB_ERR_STATE);
-  CHECK(bnb_set_tuning(h, 1, 0), BNB_ERR_ARG);
+  CHECK(bnb_set_tuning(h, 0, 0), BNB_ERR_ARG);                       /* 1..32 tiles per work item */
   CHECK(bnb_set_tuning(h, 4, 3), BNB_OK);
   CHECK(bnb_destroy(h), BNB_OK);
   memset(&empty, 0, sizeof(empty));
