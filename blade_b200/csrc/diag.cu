@@ -1,8 +1,8 @@
 // FP32 issue-rate microbenchmark: the roofline denominator of the pair kernel.
 //
 // The direct-space pair kernel runs on the FP32/MUFU pipes, not on tensor
-// cores or HBM, and the measured-peak file of the pool lists only HBM copy
-// and BF16 GEMM rates.  This kernel measures the FP32 FMA throughput of the
+// cores or HBM, so neither a copy bandwidth nor a BF16 GEMM rate bounds it.
+// This kernel measures the FP32 FMA throughput of the
 // device with 8 independent dependency chains per thread and a grid of
 // 8 CTAs x 256 threads per SM, timed with CUDA events.
 #include <cuda_runtime.h>

@@ -169,14 +169,24 @@ int bnb_compute(bnb_handle *h, const float *position, const float *lambda,
  *            sorted ascending, every pair listed from both ends
  *   out      as bnb_compute (force, energy ADDED; force64, energy64
  *            OVERWRITTEN; the energy arrays have one entry; the lambda
- *            outputs are not written)
+ *            outputs are not written).  With calcEnergy == 0, energy is
+ *            left as it was and energy64 is set to 0.
+ *
+ * Non-finite input: there is no status word.  A NaN or infinite coordinate
+ * or parameter makes the forces of the atoms it meets meaningless (the
+ * fixed-point conversion of a non-finite value is not flagged) while the
+ * call still returns 0; check the inputs beforehand when they can be
+ * non-finite, or use a handle, whose bnb_status reports them.
  *
  * Limit: atomCount <= BNB_NOALLOC_MAX_ATOMS; a larger system returns
  * BNB_ERR_TOO_LARGE and launches nothing (use a handle for it).
  * Set-up: the first call on each device looks up the device address of the
  * scratch array with that device current (cudaGetSymbolAddress; this may
  * also load the library's device code on that device); make that first call
- * before any stream capture begins.  Later calls on the device reuse it.
+ * before any stream capture begins.  Later calls on the device reuse it, so
+ * every call must run in the device's primary context (the one the CUDA
+ * runtime uses): resetting the device (cudaDeviceReset) after the first call,
+ * or calling from another driver-API context on the device, is not supported.
  * Scratch state: the array keeps what the last call left in it; each call
  * first clears, on its stream, the entries it accumulates into.
  * Concurrency: all calls on one device share the one array.  Calls that may
@@ -358,8 +368,8 @@ int bnb_lambda_histogram(int blockCount, const double *lambda, const uint8_t *bl
                          unsigned int *hist2, unsigned int *endCount, void *stream);
 
 /*
- * Autotuner: times every (tiles per work item in {4,8,16,32}) x (CTAs per SM
- * in {auto,2,3}) setting on the caller's coordinates (median of `reps`
+ * Autotuner: times every (tiles per work item in {1,2,4,8,16,32}) x (CTAs per
+ * SM in {auto,2,3}) setting on the caller's coordinates (median of `reps`
  * evaluations, CUDA events), keeps the fastest and rebuilds the list with it.
  * Synchronises.  bestMs: the kept setting's pair-evaluation time.
  */
@@ -447,7 +457,6 @@ int bnb_holonomic_position(const bnb_constraints *cs, const double *xPrev, doubl
 int bnb_holonomic_velocity(const bnb_constraints *cs, const double *x, double *v, const double *ism,
                            void *stream);
 
-/* Library version string. */
 /* ---- BF16 MLP of learned landscape flattening (no reference counterpart;
  * BLaDE's src/mlp is TorchANI inference, unrelated).  Row-major arrays,
  * BF16 as uint16_t bit patterns, products with BF16 operands and FP32
@@ -475,6 +484,7 @@ int bnb_mlp_adam(int n, float *master, uint16_t *weightBf16, const float *grad, 
 /* y = bf16(x), round to nearest even. */
 int bnb_to_bf16(int n, const float *x, uint16_t *y, void *stream);
 
+/* Library version string. */
 const char *bnb_version(void);
 
 #ifdef __cplusplus

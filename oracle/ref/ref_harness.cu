@@ -17,7 +17,10 @@
 // ref_evaluate_pme getforce_ewald / getforce_ewaldself (src/nbrecip/nbrecip.cu)
 // on PME grids set up as Potential::initialize does (potential.cxx:1202-1300),
 // and ref_holonomic holonomic_position / holonomic_velocity
-// (src/holonomic/holonomic.cu) on given constraint clusters.
+// (src/holonomic/holonomic.cu) on given constraint clusters.  The MSLD entry
+// points call Msld::calc_lambda_from_theta, calc_thetaForce_from_lambdaForce
+// and getforce_fixedBias / getforce_variableBias (src/msld/msld.cu:863-1153),
+// and ref_update_step one State::update (src/update/update.cu:233-305).
 #include <cuda_runtime.h>
 #include <cufft.h>
 
@@ -28,6 +31,7 @@
 #include <cstring>
 #include <map>
 #include <new>
+#include <string>
 
 #include "bonded/pair.h"
 #include "domdec/domdec.h"
@@ -38,6 +42,7 @@
 #include "holonomic/holonomic.h"
 #include "run/run.h"
 #include "system/potential.h"
+#include "system/selections.h"
 #include "system/state.h"
 #include "system/system.h"
 
@@ -503,6 +508,178 @@ extern "C" int ref_holonomic(ref_handle *h, int which, int nTri, const void *tri
   cudaFree(xp_d);
   cudaFree(v_d);
   cudaFree(ism_d);
+  cudaFree(pot->triangleCons_d);
+  cudaFree(pot->branch1Cons_d);
+  cudaFree(pot->branch2Cons_d);
+  cudaFree(pot->branch3Cons_d);
+  return rc ? rc : (cudaGetLastError() == cudaSuccess ? 0 : 2);
+}
+
+// ---- MSLD lambda maps, biases and the integrator step -----------------------
+// Out-of-path symbols that src/msld/msld.cu (its script parser) and
+// src/update/update.cu (the barostat) reference; never called here.
+void io_nexta(char *, char *) { fatal(__FILE__, __LINE__, "parser not available\n"); }
+std::string io_nexts(char *) { fatal(__FILE__, __LINE__, "parser not available\n"); return std::string(); }
+bool io_nextb(char *) { fatal(__FILE__, __LINE__, "parser not available\n"); return false; }
+int io_nexti(char *) { fatal(__FILE__, __LINE__, "parser not available\n"); return 0; }
+real io_nextf(char *) { fatal(__FILE__, __LINE__, "parser not available\n"); return 0; }
+void Selections::dump() {}
+void pressure_coupling(System *) { fatal(__FILE__, __LINE__, "barostat not available\n"); }
+
+// MSLD layout and biases into Msld, as Msld::initialize leaves them
+// (src/msld/msld.cu): siteBound[siteCount+1], lambdaSite[nL], blockFixed[nL]
+// (bytes), lambdaBias[nL] (the fixed bias b_i), the VariableBias list, fnex.
+extern "C" int ref_set_msld(ref_handle *h, int siteCount, const int *siteBound, const int *lambdaSite,
+                            const unsigned char *blockFixed, const float *lambdaBias, int varCount,
+                            const void *varBias, float fnex) {
+  Msld *m = h->msld;
+  const int nL = h->nL;
+  m->siteCount = siteCount;
+  m->blockCount = nL;
+  m->fnex = fnex;
+  m->fix = false;
+  m->new_implicit = false;
+  cudaMalloc(&m->siteBound_d, sizeof(int) * (siteCount + 1));
+  cudaMemcpy(m->siteBound_d, siteBound, sizeof(int) * (siteCount + 1), cudaMemcpyHostToDevice);
+  cudaMalloc(&m->lambdaSite_d, sizeof(int) * nL);
+  cudaMemcpy(m->lambdaSite_d, lambdaSite, sizeof(int) * nL, cudaMemcpyHostToDevice);
+  cudaMalloc(&m->blockFixed_d, sizeof(bool) * nL);
+  cudaMemcpy(m->blockFixed_d, blockFixed, sizeof(bool) * nL, cudaMemcpyHostToDevice);
+  cudaMalloc(&m->lambdaBias_d, sizeof(real) * nL);
+  cudaMemcpy(m->lambdaBias_d, lambdaBias, sizeof(real) * nL, cudaMemcpyHostToDevice);
+  m->variableBiasCount = varCount;
+  cudaMalloc(&m->variableBias_d, sizeof(VariableBias) * (varCount > 0 ? varCount : 1));
+  if (varCount) cudaMemcpy(m->variableBias_d, varBias, sizeof(VariableBias) * varCount, cudaMemcpyHostToDevice);
+  m->theta0_d = NULL;
+  m->dcdt_d = NULL;
+  h->run->calcTermFlag[eelambda] = true;
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// Msld::calc_lambda_from_theta on theta (host double [nL]); lambda out
+// (host double [nL]).
+extern "C" int ref_msld_lambda(ref_handle *h, const double *theta, double *lambda) {
+  State *st = h->st;
+  cudaMemcpy(st->theta_d, theta, sizeof(double) * h->nL, cudaMemcpyHostToDevice);
+  h->msld->calc_lambda_from_theta(h->stream, h->sys);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return 2;
+  cudaMemcpy(lambda, st->lambda_d, sizeof(double) * h->nL, cudaMemcpyDeviceToHost);
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// Msld::calc_thetaForce_from_lambdaForce on the FP32 mirrors lambda_fd,
+// theta_fd and lambdaForce_d (host float [nL] each); thetaForce_d starts at
+// zero and is returned (host float [nL]).
+extern "C" int ref_msld_theta_force(ref_handle *h, const float *lambda_f, const float *theta_f,
+                                    const float *lambdaForce, float *thetaForce) {
+  State *st = h->st;
+  const int nL = h->nL;
+  cudaMemcpy(st->lambda_fd, lambda_f, sizeof(float) * nL, cudaMemcpyHostToDevice);
+  cudaMemcpy(st->theta_fd, theta_f, sizeof(float) * nL, cudaMemcpyHostToDevice);
+  cudaMemcpy(st->lambdaForce_d, lambdaForce, sizeof(float) * nL, cudaMemcpyHostToDevice);
+  cudaMemset(st->thetaForce_d, 0, sizeof(float) * nL);
+  h->msld->calc_thetaForce_from_lambdaForce(h->stream, h->sys);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return 2;
+  cudaMemcpy(thetaForce, st->thetaForce_d, sizeof(float) * nL, cudaMemcpyDeviceToHost);
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// Msld::getforce_fixedBias + getforce_variableBias on lambda_fd (host float
+// [nL]); lambdaForce_d and energy_d[eelambda] start at zero and are returned.
+extern "C" int ref_msld_bias(ref_handle *h, const float *lambda_f, int calcEnergy, float *lambdaForce,
+                             double *energy) {
+  State *st = h->st;
+  const int nL = h->nL;
+  cudaMemcpy(st->lambda_fd, lambda_f, sizeof(float) * nL, cudaMemcpyHostToDevice);
+  cudaMemset(st->lambdaForce_d, 0, sizeof(float) * nL);
+  cudaMemset(st->energy_d, 0, sizeof(double) * eeend);
+  h->msld->getforce_fixedBias(h->sys, calcEnergy != 0);
+  h->msld->getforce_variableBias(h->sys, calcEnergy != 0);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return 2;
+  cudaMemcpy(lambdaForce, st->lambdaForce_d, sizeof(float) * nL, cudaMemcpyDeviceToHost);
+  if (energy) cudaMemcpy(energy, st->energy_d + eelambda, sizeof(double), cudaMemcpyDeviceToHost);
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// One State::update (src/update/update.cu:233-305) on a step that is not an
+// energy step: dU/dtheta from dU/dlambda, update_VVhbpR, holonomic_position,
+// update_OOhbpR, holonomic_position, lambda from theta.  The Msld layout must
+// be set (ref_set_msld).  Host arrays in the reference's precisions:
+//   pos    double [nL + 3N + nL]  [lambda | x | theta] in/out
+//   vel    float [3N + nL]        velocityBuffer_d (x then theta) in/out
+//   frc    float [nL + 3N + nL]   [dU/dlambda | dU/dx | dU/dtheta]; the theta
+//                                 part is added to by the step (returned)
+//   ism    float [3N + nL]        1/sqrt(m)
+//   random float [3N + nL]        the Gaussian numbers update_OOhbpR reads
+//   lp     float [6]              friction, noise, halfdt for x then theta
+// Constraint clusters as in ref_holonomic (counts may be zero).
+extern "C" int ref_update_step(ref_handle *h, double *pos, float *vel, float *frc, const float *ism,
+                               const float *random, const float *lp, int nTri, const void *tri, int n1,
+                               const void *b1, int n2, const void *b2, int n3, const void *b3, float tolerance) {
+  System *sys = h->sys;
+  State *st = h->st;
+  Potential *pot = h->pot;
+  Run *run = h->run;
+  const int N = h->N, nL = h->nL;
+  const int nbuf = 3 * N + 2 * nL, ndof = 3 * N + nL;
+  pot->triangleConsCount = nTri;
+  pot->branch1ConsCount = n1;
+  pot->branch2ConsCount = n2;
+  pot->branch3ConsCount = n3;
+  cudaMalloc(&pot->triangleCons_d, sizeof(TriangleCons) * (nTri > 0 ? nTri : 1));
+  cudaMalloc(&pot->branch1Cons_d, sizeof(Branch1Cons) * (n1 > 0 ? n1 : 1));
+  cudaMalloc(&pot->branch2Cons_d, sizeof(Branch2Cons) * (n2 > 0 ? n2 : 1));
+  cudaMalloc(&pot->branch3Cons_d, sizeof(Branch3Cons) * (n3 > 0 ? n3 : 1));
+  if (nTri) cudaMemcpy(pot->triangleCons_d, tri, sizeof(TriangleCons) * nTri, cudaMemcpyHostToDevice);
+  if (n1) cudaMemcpy(pot->branch1Cons_d, b1, sizeof(Branch1Cons) * n1, cudaMemcpyHostToDevice);
+  if (n2) cudaMemcpy(pot->branch2Cons_d, b2, sizeof(Branch2Cons) * n2, cudaMemcpyHostToDevice);
+  if (n3) cudaMemcpy(pot->branch3Cons_d, b3, sizeof(Branch3Cons) * n3, cudaMemcpyHostToDevice);
+  run->shakeTolerance = tolerance;
+  run->step = 1;
+  run->freqNRG = 1000;  // step % freqNRG != 0: the VVhbpR branch
+  run->freqNPT = 0;
+  cudaMemcpy(st->positionBuffer_d, pos, sizeof(double) * nbuf, cudaMemcpyHostToDevice);
+  cudaMemcpy(st->forceBuffer_d, frc, sizeof(float) * nbuf, cudaMemcpyHostToDevice);
+  float *v_d, *ism_d, *rnd_d;
+  cudaMalloc(&v_d, sizeof(float) * ndof);
+  cudaMalloc(&ism_d, sizeof(float) * ndof);
+  cudaMalloc(&rnd_d, sizeof(float) * ndof);
+  cudaMalloc(&st->positionCons_d, sizeof(double) * ndof);
+  cudaMalloc(&st->nanFlag_d, sizeof(int));
+  cudaMemset(st->nanFlag_d, 0xFF, sizeof(int));
+  cudaMemcpy(v_d, vel, sizeof(float) * ndof, cudaMemcpyHostToDevice);
+  cudaMemcpy(ism_d, ism, sizeof(float) * ndof, cudaMemcpyHostToDevice);
+  cudaMemcpy(rnd_d, random, sizeof(float) * ndof, cudaMemcpyHostToDevice);
+  LeapState ls;
+  memset(&ls, 0, sizeof(ls));
+  ls.N1 = 3 * N;
+  ls.N = ndof;
+  ls.x = (real_x *)st->position_d;
+  ls.v = v_d;
+  ls.f = (real_f *)st->force_d;
+  ls.ism = ism_d;
+  ls.random = rnd_d;
+  LeapParms2 lpx = {lp[0], lp[1], lp[2]}, lpt = {lp[3], lp[4], lp[5]};
+  st->leapState = &ls;
+  st->leapParms2 = &lpx;
+  st->lambdaLeapParms2 = &lpt;
+  sys->id = 0;
+  st->broadcast_position(sys);  // FP32 mirrors the theta force reads
+  st->update(1, sys);
+  int rc = cudaStreamSynchronize(h->stream) == cudaSuccess ? 0 : 2;
+  cudaMemcpy(pos, st->positionBuffer_d, sizeof(double) * nbuf, cudaMemcpyDeviceToHost);
+  cudaMemcpy(frc, st->forceBuffer_d, sizeof(float) * nbuf, cudaMemcpyDeviceToHost);
+  cudaMemcpy(vel, v_d, sizeof(float) * ndof, cudaMemcpyDeviceToHost);
+  st->leapState = NULL;
+  st->leapParms2 = NULL;
+  st->lambdaLeapParms2 = NULL;
+  cudaFree(v_d);
+  cudaFree(ism_d);
+  cudaFree(rnd_d);
+  cudaFree(st->positionCons_d);
+  cudaFree(st->nanFlag_d);
+  st->positionCons_d = NULL;
+  st->nanFlag_d = NULL;
   cudaFree(pot->triangleCons_d);
   cudaFree(pot->branch1Cons_d);
   cudaFree(pot->branch2Cons_d);

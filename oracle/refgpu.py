@@ -1,5 +1,6 @@
 """ctypes front end of oracle/_ref/libbladeref.so: the reference's own CUDA
-direct-space path (src/nbdirect + src/domdec, unmodified) driven by
+direct-space path (src/nbdirect + src/domdec, unmodified), its pair lists,
+PME, constraints, MSLD maps and biases and its integrator step, driven by
 oracle/ref/ref_harness.cu.  Comparison and golden-vector infrastructure only.
 """
 from __future__ import annotations
@@ -34,6 +35,11 @@ def lib():
         L.ref_evaluate_pme.argtypes = [p, i, i, p, p, p]
         L.ref_time_pme.argtypes = [p, i, i, p]
         L.ref_holonomic.argtypes = [p, i, i, p, i, p, i, p, i, p, p, p, p, p, f, f]
+        L.ref_set_msld.argtypes = [p, i, p, p, p, p, i, p, f]
+        L.ref_msld_lambda.argtypes = [p, p, p]
+        L.ref_msld_theta_force.argtypes = [p, p, p, p, p]
+        L.ref_msld_bias.argtypes = [p, p, i, p, p]
+        L.ref_update_step.argtypes = [p, p, p, p, p, p, p, i, p, i, p, i, p, i, p, f]
         _lib = L
     return _lib
 
@@ -168,3 +174,78 @@ def holonomic(which, tri, b1, b2, b3, x_prev, x, v, ism, halfdt, tolerance):
     if rc != 0:
         raise RuntimeError("reference harness: holonomic failed")
     return xo.reshape(-1, 3), vo.reshape(-1, 3)
+
+
+class RefMsld:
+    """The reference's Msld lambda maps, biases and State::update step on a
+    given MSLD layout (ref_set_msld, ref_msld_*, ref_update_step)."""
+
+    def __init__(self, site_bound, lambda_site, fnex=5.5, fixed=None, fixed_bias=None, var_bias=None,
+                 n_atoms=1, box=(100.0, 100.0, 100.0)):
+        from blade_b200.msld import VARBIAS_DTYPE
+        self.nL = len(lambda_site)
+        self.N = n_atoms
+        P = lambda a: a.ctypes.data_as(C.c_void_p)
+        z = np.zeros(n_atoms, np.int32)
+        zf = np.zeros(n_atoms, np.float32)
+        vdw = np.zeros(2, np.float32)
+        b = np.ascontiguousarray(box, np.float64)
+        h = C.c_void_p()
+        if lib().ref_create(n_atoms, P(z), P(zf), P(z), 1, P(vdw), 0, None, self.nL, 0, 9.0, 8.0, 0.34, 1, 0, 2.0,
+                            P(b), C.byref(h)) != 0:
+            raise RuntimeError("reference harness: create failed")
+        self.h = h
+        self._sb = np.ascontiguousarray(site_bound, np.int32)
+        self._ls = np.ascontiguousarray(lambda_site, np.int32)
+        self._fx = np.ascontiguousarray(np.zeros(self.nL) if fixed is None else fixed, np.uint8)
+        self._fb = np.ascontiguousarray(np.zeros(self.nL) if fixed_bias is None else fixed_bias, np.float32)
+        self._vb = np.ascontiguousarray(np.zeros(0, VARBIAS_DTYPE) if var_bias is None else var_bias, VARBIAS_DTYPE)
+        rc = lib().ref_set_msld(self.h, len(self._sb) - 1, P(self._sb), P(self._ls), P(self._fx), P(self._fb),
+                                len(self._vb), P(self._vb) if len(self._vb) else None, float(fnex))
+        if rc != 0:
+            raise RuntimeError("reference harness: set_msld failed")
+
+    def lambda_from_theta(self, theta):
+        th = np.ascontiguousarray(theta, np.float64)
+        lam = np.zeros(self.nL)
+        if lib().ref_msld_lambda(self.h, th.ctypes.data_as(C.c_void_p), lam.ctypes.data_as(C.c_void_p)) != 0:
+            raise RuntimeError("reference harness: msld_lambda failed")
+        return lam
+
+    def theta_force(self, lam_f, theta_f, lforce_f):
+        a = [np.ascontiguousarray(x, np.float32) for x in (lam_f, theta_f, lforce_f)]
+        out = np.zeros(self.nL, np.float32)
+        P = lambda x: x.ctypes.data_as(C.c_void_p)
+        if lib().ref_msld_theta_force(self.h, P(a[0]), P(a[1]), P(a[2]), P(out)) != 0:
+            raise RuntimeError("reference harness: msld_theta_force failed")
+        return out
+
+    def bias(self, lam_f, energy=True):
+        lf = np.ascontiguousarray(lam_f, np.float32)
+        out = np.zeros(self.nL, np.float32)
+        e = np.zeros(1)
+        P = lambda x: x.ctypes.data_as(C.c_void_p)
+        if lib().ref_msld_bias(self.h, P(lf), int(energy), P(out), P(e)) != 0:
+            raise RuntimeError("reference harness: msld_bias failed")
+        return out, float(e[0])
+
+    def update_step(self, pos, vel, frc, ism, random, lp, tri=None, b1=None, b2=None, b3=None, tolerance=2e-7):
+        """One State::update (non-energy step): returns (pos, vel, frc) after
+        the step, in the layouts documented at ref_update_step."""
+        from blade_b200.holonomic import TRI_DTYPE, B1_DTYPE, B2_DTYPE, B3_DTYPE
+        pos = np.ascontiguousarray(pos, np.float64).copy()
+        vel = np.ascontiguousarray(vel, np.float32).copy()
+        frc = np.ascontiguousarray(frc, np.float32).copy()
+        ism = np.ascontiguousarray(ism, np.float32)
+        rnd = np.ascontiguousarray(random, np.float32)
+        lp = np.ascontiguousarray(lp, np.float32)
+        arrs = [np.ascontiguousarray(np.zeros(0, dt) if a is None else a, dt)
+                for a, dt in ((tri, TRI_DTYPE), (b1, B1_DTYPE), (b2, B2_DTYPE), (b3, B3_DTYPE))]
+        P = lambda x: x.ctypes.data_as(C.c_void_p)
+        ptr = lambda x: P(x) if len(x) else None
+        rc = lib().ref_update_step(self.h, P(pos), P(vel), P(frc), P(ism), P(rnd), P(lp), len(arrs[0]), ptr(arrs[0]),
+                                   len(arrs[1]), ptr(arrs[1]), len(arrs[2]), ptr(arrs[2]), len(arrs[3]),
+                                   ptr(arrs[3]), float(tolerance))
+        if rc != 0:
+            raise RuntimeError("reference harness: update_step failed")
+        return pos, vel, frc

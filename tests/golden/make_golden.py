@@ -19,7 +19,11 @@ for the water box (orders 4, 6, 8), the MSLD water box and a small
 chain-in-water system (--pme-only makes just these); and, from the
 reference's holonomic_position / holonomic_velocity
 (src/holonomic/holonomic.cu), holonomic_*.npz for rigid waters and
-X-H groups of one to three hydrogens (--holonomic-only makes just these).
+X-H groups of one to three hydrogens (--holonomic-only makes just these);
+and, from the reference's Msld::calc_lambda_from_theta,
+calc_thetaForce_from_lambdaForce, getforce_fixedBias / getforce_variableBias
+(src/msld/msld.cu:863-1153) and State::update (src/update/update.cu:233-305),
+msld_maps*.npz and update_msld_water.npz (--msld-only makes just these).
 """
 import os
 import sys
@@ -87,10 +91,99 @@ def holonomic_cases(out):
         print(name, len(T), len(B1), len(B2), len(B3), flush=True)
 
 
-def main(out, pairs_only=False, pme_only=False, holonomic_only=False):
+MSLD_BOUND = np.array([0, 1, 5, 9, 13], np.int32)          # environment + 3 sites x 4 substituents
+MSLD_SITE = np.repeat(np.arange(4), np.diff(MSLD_BOUND)).astype(np.int32)
+
+
+def msld_varbias(rng):
+    """Every variable-bias type the reference evaluates (1-12) on pairs of
+    substituents of one site and across sites, parameters in their usual
+    ranges (k in kcal/mol; l0 the soft-core offset or the exponent)."""
+    from blade_b200.msld import VARBIAS_DTYPE
+    spec = [(6, 0.0, 0), (8, 0.017, 0), (10, -5.56, 0), (1, 0.8, 2), (2, 0.2, 2), (3, 0.0, 2), (4, 0.5, 0),
+            (5, 0.0, 0), (7, 0.1, 0), (9, 0.5, 3), (11, 2.0, 2), (12, 0.1, 2), (1, 0.8, 3), (3, 0.0, 3)]
+    vb = np.zeros(len(spec) * 2, VARBIAS_DTYPE)
+    for k, (t, l0, n) in enumerate(spec):
+        for r in range(2):
+            a = 1 + rng.integers(0, 12)
+            b = 1 + rng.integers(0, 12)
+            while b == a:
+                b = 1 + rng.integers(0, 12)
+            vb[2 * k + r] = (a, b, t, l0, rng.uniform(-4, 4), n)
+    return vb
+
+
+def msld_cases(out):
+    """Msld::calc_lambda_from_theta, calc_thetaForce_from_lambdaForce and the
+    fixed + variable biases of the reference on one layout, with and without
+    a fixed block; 16 seeded theta vectors each."""
+    rng = np.random.default_rng(11)
+    for name, fixed_blocks in (("msld_maps", ()), ("msld_maps_fixed", (6,))):
+        fixed = np.zeros(13, np.uint8)
+        for b in fixed_blocks:
+            fixed[b] = 1
+        fb = rng.normal(0, 3, 13).astype(np.float32)
+        fb[0] = 0
+        vb = msld_varbias(rng)
+        ref = refgpu.RefMsld(MSLD_BOUND, MSLD_SITE, 5.5, fixed, fb, vb)
+        th = rng.uniform(-np.pi, np.pi, (16, 13))
+        th[:, 6] = np.where(fixed[6], 0.15, th[:, 6])           # a fixed block holds its lambda in theta
+        lam = np.stack([ref.lambda_from_theta(t) for t in th])
+        lforce = rng.normal(0, 20, (16, 13)).astype(np.float32)
+        tforce = np.stack([ref.theta_force(lam[k].astype(np.float32), th[k].astype(np.float32), lforce[k])
+                           for k in range(16)])
+        bias = [ref.bias(lam[k].astype(np.float32)) for k in range(16)]
+        np.savez_compressed(os.path.join(out, name + ".npz"), site_bound=MSLD_BOUND, lambda_site=MSLD_SITE,
+                            fixed=fixed, fnex=np.float64(5.5), theta=th, lambda_ref=lam,
+                            lambda_force=lforce, theta_force_ref=tforce, fixed_bias=fb,
+                            var_bias=vb.view(np.uint8), bias_lambda_force_ref=np.stack([b[0] for b in bias]),
+                            bias_energy_ref=np.array([b[1] for b in bias]))
+        print(name, lam[0][:5], tforce[0][:5], bias[0][1], flush=True)
+
+
+def update_cases(out):
+    """One State::update of the reference (VVhbpR, SETTLE, OOhbpR, SETTLE,
+    theta forces before and lambdas after) on the MSLD water box with rigid
+    waters, friction on and the Gaussian numbers set to zero."""
+    from blade_b200 import batch, holonomic
+    s = systems.msld_water()
+    N, nL = s.N, s.msld.blockCount
+    rng = np.random.default_rng(12)
+    ox = batch.water_oxygens(s)
+    tri = holonomic.water_triangles(0, len(ox))
+    tri["idx"] = (ox[:, None] + np.arange(3)[None, :]).astype(np.int32)
+    m = batch.atom_masses(s, repartition=False)
+    kT = batch.KB * 300.0
+    theta_mass = batch.THETA_MASS
+    vx = (rng.normal(size=(N, 3)) * np.sqrt(kT / m)[:, None]).reshape(-1)
+    vt = rng.normal(size=nL) * np.sqrt(kT / theta_mass)
+    th = s.msld.theta.copy()
+    ref = refgpu.RefMsld(s.msld.siteBound, s.msld.lambdaSite, s.msld.fnex, n_atoms=N, box=s.box)
+    lam = ref.lambda_from_theta(th)
+    pos = np.concatenate([lam, s.xyz.astype(np.float64).reshape(-1), th])
+    vel = np.concatenate([vx, vt]).astype(np.float32)
+    fx = rng.normal(0, 5, 3 * N)
+    lf = rng.normal(0, 10, nL)
+    frc = np.concatenate([lf, fx, np.zeros(nL)]).astype(np.float32)
+    ism = np.concatenate([np.repeat(1 / np.sqrt(m), 3), np.full(nL, 1 / np.sqrt(theta_mass))]).astype(np.float32)
+    dt = 0.002 * batch.PICOSECOND
+    a, at = np.exp(-1.0 / batch.PICOSECOND * dt), np.exp(-5.0 / batch.PICOSECOND * dt)
+    lp = np.array([a, 0.0, 0.5 * dt, at, 0.0, 0.5 * dt], np.float32)
+    p2, v2, f2 = ref.update_step(pos, vel, frc, ism, np.zeros(3 * N + nL, np.float32), lp, tri=tri, tolerance=2e-7)
+    np.savez_compressed(os.path.join(out, "update_msld_water.npz"), pos_in=pos, vel_in=vel, frc_in=frc, ism=ism,
+                        lp=lp, tri=tri.view(np.uint8), site_bound=s.msld.siteBound, lambda_site=s.msld.lambdaSite,
+                        fnex=np.float64(s.msld.fnex), pos_ref=p2, vel_ref=v2, frc_ref=f2, n_atoms=np.int64(N))
+    print("update_msld_water", N, nL, np.abs(p2 - pos).max(), flush=True)
+
+
+def main(out, pairs_only=False, pme_only=False, holonomic_only=False, msld_only=False):
     os.makedirs(out, exist_ok=True)
     if holonomic_only:
         holonomic_cases(out)
+        return
+    if msld_only:
+        msld_cases(out)
+        update_cases(out)
         return
     for name, s, order, K in pme_cases():
         ref = refgpu.RefGPU(s)
@@ -129,4 +222,5 @@ def main(out, pairs_only=False, pme_only=False, holonomic_only=False):
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     main(args[0] if args else os.path.join(ROOT, "golden_out"), pairs_only="--pairs-only" in sys.argv,
-         pme_only="--pme-only" in sys.argv, holonomic_only="--holonomic-only" in sys.argv)
+         pme_only="--pme-only" in sys.argv, holonomic_only="--holonomic-only" in sys.argv,
+         msld_only="--msld-only" in sys.argv)

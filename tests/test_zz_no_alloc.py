@@ -9,7 +9,11 @@ in a fixed array inside the library.
 This file is collected last on purpose: it must also pass after every other
 GPU test has run in the same process.  Two calls in a row must each match
 bnb_compute within tolerance and match each other bit for bit (the second
-call runs on the scratch the first one left behind).
+call runs on the scratch the first one left behind).  Each case is also
+checked against the FP64 oracle directly, since the all-pairs kernel has its
+own minimum image and exclusion search; the output rule (force and energy
+added to, force64 and energy64 overwritten) is checked on prefilled buffers,
+and two calls on two streams ordered by an event must give the same bits.
 """
 import ctypes as C
 
@@ -17,6 +21,7 @@ import numpy as np
 import pytest
 import torch
 
+import oracle
 from blade_b200 import _lib, systems
 from blade_b200.nbdirect import NbDirect, params_for
 
@@ -25,6 +30,8 @@ pytestmark = pytest.mark.gpu
 MAX_ATOMS = 4096                  # BNB_NOALLOC_MAX_ATOMS in include/bnb.h
 FORCE_RMS_TOL = 2e-5              # relative RMS of dU/dx vs bnb_compute
 ENERGY_TOL = 2e-5                 # relative energy difference vs bnb_compute
+ORACLE_FORCE_TOL = 1e-5           # relative RMS of dU/dx vs the FP64 oracle
+ORACLE_ENERGY_TOL = 1e-5          # relative energy difference vs the FP64 oracle
 
 
 def _p(t):
@@ -110,6 +117,65 @@ def test_two_calls_match_handle_path(cuda, case):
         results.append((g, en))
     assert np.array_equal(results[0][0], results[1][0])
     assert results[0][1] == results[1][1]
+    o = oracle.nbdirect(s)
+    g_o = o["grad"].reshape(-1)
+    rel = np.sqrt(((results[0][0] - g_o) ** 2).sum() / (g_o ** 2).sum())
+    assert rel <= ORACLE_FORCE_TOL, (case, "oracle", rel)
+    assert abs(results[0][1] - o["energy"]) <= ORACLE_ENERGY_TOL * abs(o["energy"]), (case, o["energy"])
+
+
+@pytest.mark.parametrize("calc_energy", [True, False])
+def test_outputs_added_and_overwritten(cuda, calc_energy):
+    """force and energy are added to what the caller's buffers hold; force64
+    and energy64 are overwritten (energy64 with 0 on a force-only call)."""
+    s = _water(1, 0)
+    inp = _Inputs(s)
+    ref64 = torch.zeros(3 * s.N, dtype=torch.float64, device="cuda")
+    refe = torch.zeros(1, dtype=torch.float64, device="cuda")
+    assert inp.call(force64=ref64, energy64=refe, calc_energy=calc_energy) == 0
+    g = torch.Generator(device="cuda").manual_seed(7)
+    pre = torch.randn(3 * s.N, generator=g, device="cuda", dtype=torch.float32) * 3.0
+    f32 = pre.clone()
+    f64 = torch.full((3 * s.N,), 1.0e30, dtype=torch.float64, device="cuda")
+    e = torch.full((1,), -123.25, dtype=torch.float64, device="cuda")
+    e64 = torch.full((1,), 4.5e20, dtype=torch.float64, device="cuda")
+    assert inp.call(force=f32, force64=f64, energy=e, energy64=e64, calc_energy=calc_energy) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(f64, ref64)
+    want = (pre.double() + ref64).float().cpu().numpy()
+    np.testing.assert_allclose(f32.cpu().numpy(), want, rtol=1e-6, atol=1e-5)
+    if calc_energy:
+        assert float(e64.cpu()[0]) == float(refe.cpu()[0]) != 0.0
+        assert float(e.cpu()[0]) == -123.25 + float(refe.cpu()[0])
+    else:
+        assert float(e64.cpu()[0]) == 0.0
+        assert float(e.cpu()[0]) == -123.25
+
+
+def test_two_streams_ordered_by_event(cuda):
+    """Calls on two streams share the scratch array; ordered by an event they
+    give the same bits as two calls on one stream."""
+    s = _small_chain()
+    inp = _Inputs(s)
+    one = torch.zeros(3 * s.N, dtype=torch.float64, device="cuda")
+    assert inp.call(force64=one) == 0
+    torch.cuda.synchronize()
+    a = torch.cuda.Stream()
+    b = torch.cuda.Stream()
+    fa = torch.zeros(3 * s.N, dtype=torch.float64, device="cuda")
+    fb = torch.zeros(3 * s.N, dtype=torch.float64, device="cuda")
+    ev = torch.cuda.Event()
+    a.wait_stream(torch.cuda.current_stream())
+    b.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(a):
+        assert inp.call(force64=fa) == 0
+        ev.record(a)
+    b.wait_event(ev)
+    with torch.cuda.stream(b):
+        assert inp.call(force64=fb) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(fa, one)
+    assert torch.equal(fb, one)
 
 
 def test_force_only_call_matches(cuda):
