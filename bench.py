@@ -11,6 +11,11 @@ rebuild on every 10th step.  pairs/s = non-excluded pairs with r < rCut (the
 oracle's count, checked against the kernel's own count) / device time.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bnb|reference]
+                    [--workload chain_water_23558|dhfr]
+
+--workload dhfr runs the reference's own test/newDHFR fixture instead (the
+protein with its 35 CHARMM LJ types, at its input's rCut 9 / rSwitch 7.5),
+which exercises the per-pair LJ table rather than the combination rule.
 
 --impl reference times the reference algorithm's CPU restatement (FP64
 oracle port, all host threads) on bounded samples of the same workload; the
@@ -37,8 +42,16 @@ REBUILD_EVERY = 10
 ENERGY_EVERY = 10            # energy on the list-rebuild steps, forces every step
 JITTER = 0.01                # A per step
 DT_FS = 2.0
-WORKLOAD = ("chain_water_23558: 2,489-atom chain + 7,023 TIP3P, 62.23 A cube, PME(beta 0.32)+VFSWITCH, "
-            "rCut 12 rSwitch 10, pad 2 A, list rebuild every 10 steps")
+WORKLOADS = {
+    "chain_water_23558": ("chain_water_23558: 2,489-atom chain + 7,023 TIP3P, 62.23 A cube, PME(beta 0.32)+"
+                          "VFSWITCH, rCut 12 rSwitch 10, pad 2 A, list rebuild every 10 steps",
+                          "synthetic (seeded chain-in-water, 23,558 atoms per GPU)"),
+    "dhfr": ("dhfr_23558: the reference's test/newDHFR (5dfr.psf/5dfr.crd, par_all22_prot, 35 LJ types), "
+             "62.23 A cube, PME(beta 0.32)+VFSWITCH, rCut 9 rSwitch 7.5 (its m.inp), pad 2 A, list rebuild "
+             "every 10 steps",
+             "the reference's own DHFR fixture (tests/golden/fixture_dhfr.npz) moved by seeded jitter"),
+}
+WORKLOAD = WORKLOADS["chain_water_23558"][0]
 
 
 def parse():
@@ -47,6 +60,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="bnb", choices=["bnb", "reference"])
+    ap.add_argument("--workload", default="chain_water_23558", choices=sorted(WORKLOADS),
+                    help="chain_water_23558 (the headline) or dhfr (the reference's own DHFR fixture)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref", action="store_true", help="skip the reference CUDA comparison leg")
@@ -59,8 +74,10 @@ def parse():
     return ap.parse_args()
 
 
-def make_system(rank: int):
+def make_system(rank: int, workload: str = "chain_water_23558"):
     from blade_b200 import systems
+    if workload == "dhfr":                       # every rank: the same protein, its own trajectory
+        return systems.load_fixture(os.path.join(ROOT, "tests", "golden", "fixture_dhfr.npz"))
     s = systems.chain_in_water(seed=2 + rank)
     return s
 
@@ -151,7 +168,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     import oracle
-    s = make_system(0)
+    s = make_system(0, args.workload)
     cores = os.cpu_count() or 1
     sampler = oracle.Sampler(s, nthreads=cores)
     x = s.xyz.astype(np.float64)
@@ -178,8 +195,8 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": "nbdirect pairs/s", "value": value, "unit": "pairs/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded chain-in-water, 23,558 atoms)",
-            "config": {"workload": WORKLOAD, "atoms": s.N, "pairs_full_eval": full},
+            "data": WORKLOADS[args.workload][1],
+            "config": {"workload": WORKLOADS[args.workload][0], "atoms": s.N, "pairs_full_eval": full},
             "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -212,7 +229,7 @@ def run_bnb(args, rank, world):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    s = make_system(rank)
+    s = make_system(rank, args.workload)
     K, W = args.steps, args.warmup
     nb = NbDirect(s, device=dev)
     stream = torch.cuda.current_stream()
@@ -387,8 +404,8 @@ def run_bnb(args, rank, world):
     line = {
         "metric": "nbdirect pairs/s", "value": value, "unit": "pairs/s", "n_gpus": world, "steps": K,
         "warmup": W, "ms_per_step": 1e3 * t_total / K, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded chain-in-water, 23,558 atoms per GPU)",
-        "config": {"workload": WORKLOAD, "atoms": s.N, "pairs_per_step": P / K, "jitter_A": JITTER,
+        "vs_baseline": None, "dtype": "f32", "data": WORKLOADS[args.workload][1],
+        "config": {"workload": WORKLOADS[args.workload][0], "atoms": s.N, "lj_types": s.nTypes, "pairs_per_step": P / K, "jitter_A": JITTER,
                    "energy_every": ENERGY_EVERY,
                    "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}",
                    "tuning": tuning},

@@ -11,6 +11,8 @@ parameter distributions of the workloads:
 * ``msld_water``    the water box plus MSLD perturbation sites
   (3 sites x 4 substituents of 8-15 atoms).
 * ``batch_replicas`` uneven chain-in-water MSLD replicas, 3k-30k atoms.
+* ``load_fixture``  the reference's own water216 and newDHFR fixtures, as the
+  golden-vector script stored them (tests/golden/fixture_*.npz).
 
 Units are AKMA (A, kcal/mol, e).  Parameters follow the reference's tables:
 TIP3P charges/LJ from ``test/toppar_water_ions/par_water_ions.prm:77-78``,
@@ -73,6 +75,7 @@ class System:
     nbex: np.ndarray | None = None       # NBEX_DTYPE excluded pairs for the PME correction
     bonds: np.ndarray | None = None      # [B,2] int32 covalent bonds (one order), for dynamics only
     bond_param: np.ndarray | None = None  # [B,2] float32 (kb, b0): U = kb/2 (r - b0)^2
+    masses: np.ndarray | None = None      # [N] amu, when the system comes with its own
 
     @property
     def N(self) -> int:
@@ -674,3 +677,27 @@ def with_pair_lists(s: System, e14fac: float = 1.0) -> System:
         nbex[n]["idx"], nbex[n]["siteBlock"], nbex[n]["qxq"] = ij, blocks, qq
     return dc.replace(s, name=s.name + "_pairs", excl=excl.astype(np.int32), nb14=nb14, nbex=nbex)
 
+
+
+def load_fixture(path: str) -> System:
+    """A System stored by the golden-vector script from one of the reference's
+    own CHARMM fixtures (test/water216, test/newDHFR): coordinates, box,
+    charges, LJ type indices and table, exclusions (each pair once, i < j;
+    both orders are restored here, as potential.cxx:1156-1163 lists them),
+    1-4 and exclusion-correction lists in the reference's layouts, bonds and
+    masses, and the cutoffs the fixture is evaluated with."""
+    z = np.load(path)
+    N = len(z["q"])
+    nb = np.zeros(N, NBOND_DTYPE)
+    nb["q"] = z["q"]
+    nb["typeIdx"] = z["typeIdx"]
+    half = z["excl_half"].astype(np.int32)
+    excl = np.concatenate([half, half[:, ::-1]])
+    excl = excl[np.lexsort((excl[:, 1], excl[:, 0]))]
+    s = System(str(z["name"]), z["xyz"].astype(np.float32), z["box"].astype(np.float32), nb,
+               z["vdw"].astype(np.float32), excl, float(z["rCut"]), float(z["rSwitch"]), float(z["beta"]))
+    s.nb14 = z["nb14"].view(NB14_DTYPE).copy()
+    s.nbex = z["nbex"].view(NBEX_DTYPE).copy()
+    s.bonds = z["bonds"].astype(np.int32)
+    s.masses = z["masses"].astype(np.float64)
+    return s

@@ -23,14 +23,19 @@ X-H groups of one to three hydrogens (--holonomic-only makes just these);
 and, from the reference's Msld::calc_lambda_from_theta,
 calc_thetaForce_from_lambdaForce, getforce_fixedBias / getforce_variableBias
 (src/msld/msld.cu:863-1153) and State::update (src/update/update.cu:233-305),
-msld_maps*.npz and update_msld_water.npz (--msld-only makes just these).
+msld_maps*.npz and update_msld_water.npz (--msld-only makes just these);
+and the reference's own CHARMM fixtures: `make_golden.py REFERENCE_ROOT
+--fixtures` (CPU) turns test/water216 and test/newDHFR into
+fixture_<name>.npz, and `--real-only` (GPU) evaluates the reference's direct
+space, nb14, nbex, PME and self terms on them into real_<name>.npz.
 """
 import os
 import sys
 
 import numpy as np
 
-ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from blade_b200 import systems  # noqa: E402
@@ -176,8 +181,55 @@ def update_cases(out):
     print("update_msld_water", N, nL, np.abs(p2 - pos).max(), flush=True)
 
 
-def main(out, pairs_only=False, pme_only=False, holonomic_only=False, msld_only=False):
+# The reference's own CHARMM fixtures with the cutoffs their inputs use:
+# test/water216/input at the 216-water configuration's 9/8 A (its default
+# 10 A cutoff exceeds half the 18.856 A box), test/newDHFR/m.inp as written
+# (rcut 9, rswitch 7.5, invbetaewald 3.125, orderewald 4, gridspace 1.1).
+REAL = {"water216": dict(rCut=9.0, rSwitch=8.0, beta=0.34, order=6, space=1.0),
+        "dhfr": dict(rCut=9.0, rSwitch=7.5, beta=0.32, order=4, space=1.1)}
+
+
+def make_fixtures(reference_root, out):
+    """CPU step (needs the reference's test/ tree, not a GPU): reads the PSF,
+    CRD and parameter files with oracle/charmm.py and stores the systems as
+    fixture_<name>.npz (blade_b200.systems.load_fixture reads them)."""
+    from oracle import charmm
+    for name, (psf, crd, prm, box) in charmm.fixture_paths(reference_root).items():
+        c = REAL[name]
+        s = charmm.build(psf, crd, prm, box, c["rCut"], c["rSwitch"], c["beta"], name)
+        charmm.save_fixture(s, os.path.join(out, f"fixture_{name}.npz"))
+        print("fixture", name, s.N, s.nTypes, len(s.excl), len(s.nb14), len(s.nbex), flush=True)
+
+
+def real_cases(out):
+    """The reference's direct space, nb14, nbex, PME reciprocal and self
+    terms on the stored fixtures (GPU step)."""
+    from oracle import pme_oracle
+    for name, c in REAL.items():
+        s = systems.load_fixture(os.path.join(HERE, f"fixture_{name}.npz"))
+        ref = refgpu.RefGPU(s)
+        r = ref.evaluate()
+        ref.set_pairs(False)
+        r14 = ref.evaluate_pairs("nb14")
+        rex = ref.evaluate_pairs("nbex")
+        K = [pme_oracle.grid_size(L, c["space"]) for L in s.box]
+        ref.set_pme(c["order"], K)
+        rp = ref.evaluate_pme("recip")
+        rs = ref.evaluate_pme("self")
+        f32 = lambda a: a.astype(np.float32)
+        np.savez_compressed(os.path.join(out, f"real_{name}.npz"), grad=f32(r["grad"]), energy=np.float64(r["energy"]),
+                            grad14=f32(r14["grad"]), energy14=np.float64(r14["energy"]),
+                            gradex=f32(rex["grad"]), energyex=np.float64(rex["energy"]),
+                            gradpme=f32(rp["grad"]), energypme=np.float64(rp["energy"]),
+                            energyself=np.float64(rs["energy"]), K=np.int64(K), order=np.int64(c["order"]))
+        print("real", name, r["energy"], r14["energy"], rex["energy"], rp["energy"], rs["energy"], K, flush=True)
+
+
+def main(out, pairs_only=False, pme_only=False, holonomic_only=False, msld_only=False, real_only=False):
     os.makedirs(out, exist_ok=True)
+    if real_only:
+        real_cases(out)
+        return
     if holonomic_only:
         holonomic_cases(out)
         return
@@ -221,6 +273,9 @@ def main(out, pairs_only=False, pme_only=False, holonomic_only=False, msld_only=
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    if "--fixtures" in sys.argv:
+        make_fixtures(args[0], args[1] if len(args) > 1 else HERE)
+        sys.exit(0)
     main(args[0] if args else os.path.join(ROOT, "golden_out"), pairs_only="--pairs-only" in sys.argv,
          pme_only="--pme-only" in sys.argv, holonomic_only="--holonomic-only" in sys.argv,
-         msld_only="--msld-only" in sys.argv)
+         msld_only="--msld-only" in sys.argv, real_only="--real-only" in sys.argv)
