@@ -178,12 +178,13 @@ __device__ __forceinline__ void lj_params(const float2 *sLJ, int rowI, int tj, f
     float R6 = R2 * R2 * R2;
     c6 = (e6 * (1.f / 6.f)) * R6;
     c12 = (e6 * (1.f / 12.f)) * R6 * R6;
-  } else {
+  } else {  // the shared table holds (12 c12, 6 c6)
     float2 v = sLJ[rowI + tj];
-    c12 = v.x;
-    c6 = v.y;
+    c12 = v.x * (1.f / 12.f);
+    c6 = v.y * (1.f / 6.f);
   }
 }
+
 
 struct KArgs {
   Dev d;
@@ -227,11 +228,13 @@ __device__ __forceinline__ float plain_pair(const PairConst &pc, float r2, float
         c6 = (e6 * (1.f / 6.f)) * R6;
         c12 = (e6 * (1.f / 12.f)) * R6 * R6;
       }
-    } else {
+    } else {  // the shared table holds (12 c12, 6 c6)
       const float2 v = sLJ[rowI + tj];
-      c12 = v.x;
-      c6 = v.y;
-      flr = fmaf(6.f * c6 * a, rinv3, -12.f * c12 * b * rinv6);
+      flr = fmaf(v.y * a, rinv3, -(v.x * b) * rinv6);
+      if (ENERGY) {
+        c12 = v.x * (1.f / 12.f);
+        c6 = v.y * (1.f / 6.f);
+      }
     }
     if (ENERGY) {
       const float pe = in ? fmaf(rinv6, rinv6, -pc.dv12) : b * (rinv6 - pc.rci6);
@@ -248,6 +251,97 @@ __device__ __forceinline__ float plain_pair(const PairConst &pc, float r2, float
     return dEdr * rinv;
   }
 }
+
+// ---------------------------------------------------------------------------
+// Packed FP32x2 arithmetic (sm_100): one instruction updates the .x and .y
+// halves, which the streamed tile path below uses for two independent pairs
+// (A in .x, B in .y) of one lane.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sel2(bool x, bool y, float2 a, float2 b) {
+  return make_float2(x ? a.x : b.x, y ? a.y : b.y);
+}
+
+// Two PME + VFSWITCH pairs at squared distances r2 (.x for pair A, .y for B):
+// returns (dE/dr)/r for both; with ENERGY also their energies.  Same
+// algebra as plain_pair<PME, VFSWITCH>: erfc(beta r) = exp(-beta^2 r^2) P6(t),
+// VFSWITCH folded outside rSwitch.  Table mode takes (12 c12, 6 c6), combine
+// mode (e6, R) = (sqrt(12 eps_i) sqrt(12 eps_j), Rmin/2_i + Rmin/2_j).
+template <bool ENERGY, bool COMBINE>
+__device__ __forceinline__ float2 pme_vfsw_pair2(const PairConst &pc, float2 r2, float2 qq, float2 lj0, float2 lj1,
+                                                 float2 &E) {
+  const float2 rinv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+  const float2 r = mul2(r2, rinv);
+  const float2 targ = fma2(f2(pc.pBeta), r, f2(1.0f));
+  const float2 t = make_float2(rcp_approx(targ.x), rcp_approx(targ.y));
+  const float2 garg = mul2(f2(pc.mBeta2Log2e), r2);
+  const float2 g = make_float2(ex2_approx(garg.x), ex2_approx(garg.y));
+  const float2 t2 = mul2(t, t);
+  float2 pe = fma2(f2(kErfcC6), t2, f2(kErfcC4));
+  pe = fma2(pe, t2, f2(kErfcC2));
+  pe = fma2(pe, t2, f2(kErfcC0));
+  float2 po = fma2(f2(kErfcC5), t2, f2(kErfcC3));
+  po = fma2(po, t2, f2(kErfcC1));
+  const float2 p = fma2(po, t, pe);
+  const float2 qg = mul2(qq, g);
+  const float2 rinv2 = mul2(rinv, rinv);
+  const float2 rinv3 = mul2(rinv2, rinv);
+  const float2 rinv6 = mul2(rinv3, rinv3);
+  const bool inA = r.x < pc.rswitch, inB = r.y < pc.rswitch;
+  const float2 a = sel2(inA, inB, rinv3, fma2(f2(pc.k6), rinv3, f2(-pc.k6rci3)));
+  const float2 b = sel2(inA, inB, rinv6, fma2(f2(pc.k12), rinv6, f2(-pc.k12rci6)));
+  float2 flr, c12, c6;
+  if (COMBINE) {  // lj0 = e6, lj1 = R
+    const float2 R2 = mul2(lj1, lj1);
+    const float2 R6 = mul2(mul2(R2, R2), R2);
+    const float2 w = mul2(R6, rinv3);
+    flr = mul2(mul2(lj0, w), fma2(mul2(w, f2(-1.f)), b, a));
+    if (ENERGY) {
+      c6 = mul2(mul2(lj0, f2(1.f / 6.f)), R6);
+      c12 = mul2(mul2(mul2(lj0, f2(1.f / 12.f)), R6), R6);
+    }
+  } else {        // lj0 = 12 c12, lj1 = 6 c6
+    flr = fma2(mul2(lj1, a), rinv3, mul2(mul2(mul2(lj0, f2(-1.f)), b), rinv6));
+    if (ENERGY) {
+      c12 = mul2(lj0, f2(1.f / 12.f));
+      c6 = mul2(lj1, f2(1.f / 6.f));
+    }
+  }
+  if (ENERGY) {
+    const float2 pe_in = fma2(rinv6, rinv6, f2(-pc.dv12));
+    const float2 pe_out = mul2(b, add2(rinv6, f2(-pc.rci6)));
+    const float2 qe_in = add2(rinv6, f2(-pc.dv6));
+    const float2 qe_out = mul2(a, add2(rinv3, f2(-pc.rci3)));
+    const float2 pe2 = sel2(inA, inB, pe_in, pe_out);
+    const float2 qe2 = sel2(inA, inB, qe_in, qe_out);
+    E = fma2(mul2(qg, p), rinv, fma2(c12, pe2, mul2(mul2(c6, qe2), f2(-1.f))));
+  }
+  // Coulomb part of (dE/dr) r: -qq g (p / r + 2 beta / sqrt(pi))
+  return mul2(fma2(mul2(qg, f2(-1.f)), fma2(p, rinv, f2(pc.twoBetaSqrtPi)), flr), rinv2);
+}
+
+
+
+// Per-lane loads of one candidate tile (its j slot for this lane).
+template <int ALCH>
+struct TileFetch {
+  int jBlock, code, mIdx, atom, siteBlock;
+  float4 xj;
+  uint32_t row;
+  __device__ __forceinline__ void fetch(const Dev &d, int4 cand, int c, int lane) {
+    jBlock = __shfl_sync(kFull, cand.x, c);
+    code = __shfl_sync(kFull, cand.y, c);
+    mIdx = __shfl_sync(kFull, cand.z, c);
+    const int jslot = 32 * jBlock + lane;
+    xj = d.xyzq[jslot];
+    atom = d.slotAtom[jslot];
+    siteBlock = ALCH ? d.slotSiteBlock[jslot] : 0;
+    row = mIdx >= 0 ? d.masks[32 * (size_t)mIdx + lane] : kFull;
+  }
+};
 
 // j-side registers that travel with the rotation.
 template <bool COMBINE, int ALCH>
@@ -322,20 +416,150 @@ __device__ __forceinline__ void plain_loop(JRegs<COMBINE, ALCH> &J, const float4
 }
 
 // ---------------------------------------------------------------------------
+// Streamed tiles.  The compacted j atoms of a work item's tiles that need no
+// exclusion mask and no MSLD scaling are queued in shared memory as entries
+// (j slot | shift code << 27) and evaluated in chunks of up to 64: every lane
+// keeps its i atom and holds two queued j atoms, A = entry cl and B = entry
+// gj + cl of its group of gj lanes (gj = 32, 16, 8 or 4 for chunks of more
+// than 32, 16, 8 or up to 8 entries; smaller groups are replicated), and the
+// pair math of A and B runs in packed FP32x2 instructions.  After gj rotation
+// steps each group lane holds the group's partial forces of its own two
+// entries; the groups are summed by xor shuffles and group 0 adds them to the
+// fixed-point accumulators, one addition per queued j atom.  A chunk costs its
+// entry count rounded up to an even number of gj-lane rotations, so a tile
+// contributes exactly its compacted j atoms and only the last chunk of a work
+// item is padded.
+// ---------------------------------------------------------------------------
+template <bool COMBINE>
+__device__ __forceinline__ void stream_load(const Dev &d, int e, float bx, float by, float bz, float &x, float &y,
+                                            float &z, float &q, int &t, float &ex, float &er) {
+  if (e < 0) {  // padding: far outside rCut of every i atom
+    x = 1.0e18f; y = 0.f; z = 0.f; q = 0.f; t = 0; ex = 0.f; er = 0.f;
+    return;
+  }
+  const int js = e & 0x7FFFFFF;
+  int sx, sy, sz;
+  shift_of(e >> 27, sx, sy, sz);
+  const float4 xj = d.xyzq[js];
+  x = xj.x + (float)sx * bx;
+  y = xj.y + (float)sy * by;
+  z = xj.z + (float)sz * bz;
+  q = xj.w;
+  t = d.slotType[js];
+  if (COMBINE) {
+    const float2 lj = d.ljType[t];
+    ex = lj.x;
+    er = lj.y;
+  }
+}
+
+template <int ELEC, int VDW, bool ENERGY, bool COMBINE>
+__device__ __forceinline__ void stream_chunk(const Dev &d, const PairConst &pc, const float2 *sLJ, const int *sS,
+                                             int C, int lane, float4 xi, int rowI, float2 ljI, float bx, float by,
+                                             float bz, float2 &fix2, float2 &fiy2, float2 &fiz2, long long &ei,
+                                             unsigned long long &pairs, int count) {
+  const int gj = C > 32 ? 32 : (C > 16 ? 16 : (C > 8 ? 8 : 4));
+  const int cl = lane & (gj - 1);
+  const int eA = cl < C ? sS[cl] : -1;
+  const int eB = gj + cl < C ? sS[gj + cl] : -1;
+  float2 jx, jy, jz, jq, jex = f2(0.f), jer = f2(0.f);
+  int tA, tB;
+  stream_load<COMBINE>(d, eA, bx, by, bz, jx.x, jy.x, jz.x, jq.x, tA, jex.x, jer.x);
+  stream_load<COMBINE>(d, eB, bx, by, bz, jx.y, jy.y, jz.y, jq.y, tB, jex.y, jer.y);
+  float2 jfx = f2(0.f), jfy = f2(0.f), jfz = f2(0.f);
+  const float2 xi2 = f2(xi.x), yi2 = f2(xi.y), zi2 = f2(xi.z), qi2 = f2(xi.w);
+  const float2 m1 = f2(-1.f);
+  const int rot = lane + 1;
+#pragma unroll 2
+  for (int k = 0; k < gj; k++) {
+    const float2 dx = fma2(jx, m1, xi2), dy = fma2(jy, m1, yi2), dz = fma2(jz, m1, zi2);
+    const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+    const bool actA = r2.x < pc.rc2, actB = r2.y < pc.rc2;
+    float2 fs, E = f2(0.f);
+    if (ELEC == 1 && VDW == 0) {
+      float2 lj0, lj1;
+      if (COMBINE) {
+        lj0 = mul2(f2(ljI.x), jex);
+        lj1 = add2(f2(ljI.y), jer);
+      } else {
+        const float2 vA = sLJ[rowI + tA], vB = sLJ[rowI + tB];
+        lj0 = make_float2(vA.x, vB.x);
+        lj1 = make_float2(vA.y, vB.y);
+      }
+      fs = pme_vfsw_pair2<ENERGY, COMBINE>(pc, r2, mul2(qi2, jq), lj0, lj1, E);
+    } else {
+      fs.x = plain_pair<ELEC, VDW, ENERGY, COMBINE>(pc, r2.x, xi.w * jq.x, sLJ, rowI, tA, ljI,
+                                                    make_float2(jex.x, jer.x), E.x);
+      fs.y = plain_pair<ELEC, VDW, ENERGY, COMBINE>(pc, r2.y, xi.w * jq.y, sLJ, rowI, tB, ljI,
+                                                    make_float2(jex.y, jer.y), E.y);
+    }
+    fs = sel2(actA, actB, fs, f2(0.f));
+    fix2 = fma2(fs, dx, fix2);
+    fiy2 = fma2(fs, dy, fiy2);
+    fiz2 = fma2(fs, dz, fiz2);
+    jfx = fma2(fs, dx, jfx);  // the j atoms' forces with the sign of the i side, negated below
+    jfy = fma2(fs, dy, jfy);
+    jfz = fma2(fs, dz, jfz);
+    if (ENERGY) {
+      if (actA) ei += to_fix(E.x);
+      if (actB) ei += to_fix(E.y);
+      if (count) pairs += (unsigned long long)actA + (unsigned long long)actB;
+    }
+    jx.x = __shfl_sync(kFull, jx.x, rot, gj); jx.y = __shfl_sync(kFull, jx.y, rot, gj);
+    jy.x = __shfl_sync(kFull, jy.x, rot, gj); jy.y = __shfl_sync(kFull, jy.y, rot, gj);
+    jz.x = __shfl_sync(kFull, jz.x, rot, gj); jz.y = __shfl_sync(kFull, jz.y, rot, gj);
+    jq.x = __shfl_sync(kFull, jq.x, rot, gj); jq.y = __shfl_sync(kFull, jq.y, rot, gj);
+    if (COMBINE) {
+      jex.x = __shfl_sync(kFull, jex.x, rot, gj); jex.y = __shfl_sync(kFull, jex.y, rot, gj);
+      jer.x = __shfl_sync(kFull, jer.x, rot, gj); jer.y = __shfl_sync(kFull, jer.y, rot, gj);
+    } else {
+      tA = __shfl_sync(kFull, tA, rot, gj); tB = __shfl_sync(kFull, tB, rot, gj);
+    }
+    jfx.x = __shfl_sync(kFull, jfx.x, rot, gj); jfx.y = __shfl_sync(kFull, jfx.y, rot, gj);
+    jfy.x = __shfl_sync(kFull, jfy.x, rot, gj); jfy.y = __shfl_sync(kFull, jfy.y, rot, gj);
+    jfz.x = __shfl_sync(kFull, jfz.x, rot, gj); jfz.y = __shfl_sync(kFull, jfz.y, rot, gj);
+  }
+  for (int o = 16; o >= gj; o >>= 1) {
+    jfx.x += __shfl_xor_sync(kFull, jfx.x, o); jfx.y += __shfl_xor_sync(kFull, jfx.y, o);
+    jfy.x += __shfl_xor_sync(kFull, jfy.x, o); jfy.y += __shfl_xor_sync(kFull, jfy.y, o);
+    jfz.x += __shfl_xor_sync(kFull, jfz.x, o); jfz.y += __shfl_xor_sync(kFull, jfz.y, o);
+  }
+  if (lane < gj) {
+    const int S = 32 * d.maxBlocks;
+    if (eA >= 0 && (jfx.x != 0.f || jfy.x != 0.f || jfz.x != 0.f)) {
+      const int js = eA & 0x7FFFFFF;
+      red_add(&d.accF[js], to_fix(-jfx.x));
+      red_add(&d.accF[S + js], to_fix(-jfy.x));
+      red_add(&d.accF[2 * S + js], to_fix(-jfz.x));
+      if (!(isfinite(jfx.x) && isfinite(jfy.x) && isfinite(jfz.x))) atomicOr(&d.ctr->status, kStatusNonFinite);
+    }
+    if (eB >= 0 && (jfx.y != 0.f || jfy.y != 0.f || jfz.y != 0.f)) {
+      const int js = eB & 0x7FFFFFF;
+      red_add(&d.accF[js], to_fix(-jfx.y));
+      red_add(&d.accF[S + js], to_fix(-jfy.y));
+      red_add(&d.accF[2 * S + js], to_fix(-jfz.y));
+      if (!(isfinite(jfx.y) && isfinite(jfy.y) && isfinite(jfz.y))) atomicOr(&d.ctr->status, kStatusNonFinite);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // The pair kernel.
 // ALCH: 0 none, 1 MSLD scaling, 2 MSLD scaling + soft core.
 //
-// Tile processing with j compaction: the j atoms of a tile that lie within
-// rCut of the i block's AABB are gathered into lanes 0..nj-1 and replicated in
-// groups of gj = 8, 16 or 32 lanes (smallest gj >= nj).  Every lane keeps its
-// own i atom and rotates through the gj compacted j atoms of its group, so a
-// tile costs gj steps instead of 32; the group partial j forces are summed
-// with xor shuffles and returned to the owner lanes.
+// Tile processing with j compaction: the nj j atoms of a tile that lie within
+// rCut of the i block's AABB are taken in chunks of gj = 32, 16, 8 or 4
+// (every chunk but the last full), each replicated in groups of gj lanes.
+// Every lane keeps its own i atom and rotates through the gj j atoms of its
+// group, so a tile costs nj rounded up to a multiple of 4 steps instead of
+// 32; the group partial j forces are summed with xor shuffles and returned to
+// the owner lanes, one chunk per j atom.
 // ---------------------------------------------------------------------------
 template <int ELEC, int VDW, int ALCH, bool ENERGY, bool COMBINE>
-__global__ void __launch_bounds__(256, (ALCH || ENERGY) ? 3 : 4) k_pair(KArgs A) {
+__global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int sIdx[8][32];
+  __shared__ int sStream[8][128];  // queued entries of streamed tiles, per warp
   const Dev &d = A.d;
   const PairConst &pc = A.pc;
   const int lane = threadIdx.x & 31;
@@ -347,8 +571,11 @@ __global__ void __launch_bounds__(256, (ALCH || ENERGY) ? 3 : 4) k_pair(KArgs A)
   long long *sAccL = reinterpret_cast<long long *>(smem + off);
   float *sLam = reinterpret_cast<float *>(smem + off + (ALCH ? sizeof(long long) * d.lamTotal : 0));
 
-  if (!COMBINE)
-    for (int i = threadIdx.x; i < nT * nT; i += blockDim.x) sLJ[i] = d.ljTable[i];
+  if (!COMBINE)  // (12 c12, 6 c6): the factors of the force expressions folded in
+    for (int i = threadIdx.x; i < nT * nT; i += blockDim.x) {
+      const float2 v = d.ljTable[i];
+      sLJ[i] = make_float2(12.f * v.x, 6.f * v.y);
+    }
   if (ALCH)
     for (int i = threadIdx.x; i < d.lamTotal; i += blockDim.x) {
       sAccL[i] = 0;
@@ -397,156 +624,206 @@ __global__ void __launch_bounds__(256, (ALCH || ENERGY) ? 3 : 4) k_pair(KArgs A)
     unsigned act = __ballot_sync(kFull, hit);
 
     float fix = 0.f, fiy = 0.f, fiz = 0.f, fli = 0.f;
+    float2 fix2 = f2(0.f), fiy2 = f2(0.f), fiz2 = f2(0.f);  // i forces of the streamed pairs (A, B)
+    int nS = 0;        // entries queued in sStream[warp]
     long long ei = 0;  // fixed-point energy of this lane's pairs
+    // The loads of each tile are issued one tile ahead, so their latency
+    // overlaps the compaction and chunk work of the tile before.
+    TileFetch<ALCH> nxt;
+    if (act) nxt.fetch(d, cand, __ffs(act) - 1, lane);
     while (act) {
-      const int c = __ffs(act) - 1;
       act &= act - 1;
-      const int jBlock = __shfl_sync(kFull, cand.x, c);
-      const int code = __shfl_sync(kFull, cand.y, c);
-      const int mIdx = __shfl_sync(kFull, cand.z, c);
+      const TileFetch<ALCH> cur = nxt;
+      if (act) nxt.fetch(d, cand, __ffs(act) - 1, lane);
+      const int jBlock = cur.jBlock;
+      const int code = cur.code;
+      const int mIdx = cur.mIdx;
       int sx, sy, sz;
       shift_of(code, sx, sy, sz);
+      const float shx = (float)sx * bx, shy = (float)sy * by, shz = (float)sz * bz;
       const int jslot = 32 * jBlock + lane;
-      JRegs<COMBINE, ALCH> J;
-      {
-        const float4 xj = d.xyzq[jslot];
-        J.x = xj.x + (float)sx * bx;
-        J.y = xj.y + (float)sy * by;
-        J.z = xj.z + (float)sz * bz;
-        J.q = xj.w;
-      }
-      const int tj = d.slotType[jslot];
-      J.meta = COMBINE ? lane : ((lane << 16) | tj);
-      if (COMBINE) {
-        const float2 lj2 = d.ljType[tj];
-        J.ex = lj2.x;
-        J.er = lj2.y;
-      }
-      const int bj0 = ALCH ? d.slotSiteBlock[jslot] : 0;
-      if (ALCH) {
-        J.b = bj0;
-        J.l = bj0 ? sLam[bj0 & 0xFFFF] : 1.f;
-      }
-      const bool jValid = d.slotAtom[jslot] >= 0;
-      uint32_t row = mIdx >= 0 ? d.masks[32 * (size_t)mIdx + lane] : kFull;
+      const float jx = cur.xj.x + shx, jy = cur.xj.y + shy, jz = cur.xj.z + shz;
+      const int bj0 = ALCH ? cur.siteBlock : 0;
+      const bool jValid = cur.atom >= 0;
+      uint32_t row = cur.row;
       if (jBlock == iBlock && code == 0) row &= (lane == 31) ? 0u : (kFull << (lane + 1));
       if (!iValid) row = 0u;
 
       // j atoms that can reach the i block (per-atom AABB test, nbdirect.cu:211)
       float g, gap2;
-      g = fmaxf(fmaxf(imin.x - J.x, J.x - imax.x), 0.f);
+      g = fmaxf(fmaxf(imin.x - jx, jx - imax.x), 0.f);
       gap2 = g * g;
-      g = fmaxf(fmaxf(imin.y - J.y, J.y - imax.y), 0.f);
+      g = fmaxf(fmaxf(imin.y - jy, jy - imax.y), 0.f);
       gap2 = fmaf(g, g, gap2);
-      g = fmaxf(fmaxf(imin.z - J.z, J.z - imax.z), 0.f);
+      g = fmaxf(fmaxf(imin.z - jz, jz - imax.z), 0.f);
       gap2 = fmaf(g, g, gap2);
       const bool jin = jValid && gap2 < pc.rc2;
       const unsigned jm = __ballot_sync(kFull, jin);
       const int nj = __popc(jm);
       if (nj == 0) continue;
-      const int gj = nj <= 8 ? 8 : (nj <= 16 ? 16 : 32);
       const bool alchTile = ALCH ? __any_sync(kFull, (bi | bj0) != 0) : false;
-
-      // compact: lane p of every group receives the p-th surviving j atom
-      const int rank = __popc(jm & ((1u << lane) - 1u));
-      if (jin) sIdx[warp][rank] = lane;
-      __syncwarp();
-      const int cl = lane & (gj - 1);
-      const int src = cl < nj ? sIdx[warp][cl] : lane;
-      __syncwarp();
-      J.move(src, 32, true, alchTile);
-      if (cl >= nj) J.x = 1.0e18f;  // empty compacted slot: never within rCut
-      J.fx = J.fy = J.fz = J.fl = 0.f;
-      const int rot = lane + 1;
       // Tiles without an exclusion mask and off the diagonal need no per-step
       // mask test: empty j slots and invalid i lanes sit far outside rCut.
       const bool masked = mIdx >= 0 || (jBlock == iBlock && code == 0);
 
-      if (!alchTile) {
-        if (masked)
-          plain_loop<ELEC, VDW, ENERGY, COMBINE, true>(J, xi, row, gj, rot, pc, sLJ, rowI, ljI, fix, fiy, fiz,
-                                                       ei, pairs, A.count);
-        else
-          plain_loop<ELEC, VDW, ENERGY, COMBINE, false>(J, xi, row, gj, rot, pc, sLJ, rowI, ljI, fix, fiy,
-                                                        fiz, ei, pairs, A.count);
-      } else if (ALCH) {
-        for (int k = 0; k < gj; k++) {
-          const float dx = xi.x - J.x, dy = xi.y - J.y, dz = xi.z - J.z;
-          const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          const int jb = COMBINE ? J.meta : (J.meta >> 16);
-          if (((row >> jb) & 1u) && r2 < pc.rc2) {
-            float c12, c6;
-            lj_params<COMBINE>(sLJ, rowI, J.meta & 0xFFFF, ljI, make_float2(J.ex, J.er), c12, c6);
-            const float rinv = rsqrt_approx(r2);
-            const float r = r2 * rinv;
-            const int bj = J.b;
-            const float lj = J.l;
-            // MSLD scaling, nbdirect.cu:244-254
-            const bool sameSite = (bi & 0xFFFF0000) == (bj & 0xFFFF0000);
-            const float s = sameSite ? (bi == bj ? li : 0.f) : li * lj;
-            const bool pert = (bi | bj) != 0;
-            float rEff = r, rinvE = rinv, r2E = r2, dredr = 1.f, dredll = 0.f;
-            if (ALCH == 2 && pert) {  // soft core, nbdirect.cu:257-275
-              const float rSoft = pc.softR * (1.f - s);
-              if (r < rSoft) {
-                const float q = __fdividef(r, rSoft);
-                const float f = fmaf(q * q * q, fmaf(-0.5f, q, 1.f), 0.5f);
-                dredr = (3.f - 2.f * q) * q * q;
-                dredll = -pc.softR * (f - dredr * q);
-                rEff = f * rSoft;
-                rinvE = rcp_approx(rEff);
-                r2E = rEff * rEff;
-              }
-            }
-            float dEdr, E;
-            pair_terms<ELEC, VDW, true>(pc, rEff, r2E, rinvE, xi.w * J.q, c12, c6, dEdr, E);
-            dEdr *= s;
-            if (pert) {  // dU/dlambda routing, nbdirect.cu:400-415
-              const float fl = fmaf(dEdr, dredll, E);
-              if (sameSite) {
-                if (bi == bj) fli += fl;
-              } else {
-                fli = fmaf(lj, fl, fli);
-                J.fl = fmaf(li, fl, J.fl);
-              }
-            }
-            const float fs = dEdr * dredr * rinv;
-            fix = fmaf(fs, dx, fix); fiy = fmaf(fs, dy, fiy); fiz = fmaf(fs, dz, fiz);
-            J.fx = fmaf(-fs, dx, J.fx); J.fy = fmaf(-fs, dy, J.fy); J.fz = fmaf(-fs, dz, J.fz);
-            if (ENERGY) ei += to_fix(s * E);
-            if (ENERGY && A.count) pairs++;
-          }
-          J.move(rot, gj);
-          J.move_forces(rot, gj, true);
+      const int rank = __popc(jm & ((1u << lane) - 1u));
+      if (!masked && !alchTile) {  // streamed: queue the compacted j atoms, evaluate full chunks of 64
+        if (jin) sStream[warp][nS + rank] = jslot | (code << 27);
+        nS += nj;
+        __syncwarp();
+        if (nS >= 64) {
+          stream_chunk<ELEC, VDW, ENERGY, COMBINE>(d, pc, sLJ, sStream[warp], 64, lane, xi, rowI, ljI, bx, by, bz,
+                                                   fix2, fiy2, fiz2, ei, pairs, A.count);
+          const int rest = nS - 64;  // < 32
+          const int carry = lane < rest ? sStream[warp][64 + lane] : 0;
+          __syncwarp();
+          if (lane < rest) sStream[warp][lane] = carry;
+          __syncwarp();
+          nS = rest;
         }
+        continue;
       }
-      // sum the group partials; group 0 lane p now holds compacted j p
-      float fx = J.fx, fy = J.fy, fz = J.fz, fl = J.fl;
-      if (gj <= 16) {
-        fx += __shfl_xor_sync(kFull, fx, 16); fy += __shfl_xor_sync(kFull, fy, 16);
-        fz += __shfl_xor_sync(kFull, fz, 16);
-        if (ALCH && alchTile) fl += __shfl_xor_sync(kFull, fl, 16);
+      // compaction order: the p-th surviving j atom is lane sIdx[p]
+      if (jin) sIdx[warp][rank] = lane;
+      __syncwarp();
+      // j force of this lane's own j atom, delivered by the chunk that held it
+      float ofx = 0.f, ofy = 0.f, ofz = 0.f, ofl = 0.f;
+      // The nj surviving j atoms are processed in chunks of 32, 16, 8 or 4
+      // (32 only when more than 28 survive; otherwise 16 while more than 12
+      // remain, then 8, then 4), each replicated in groups of gj lanes, so a
+      // tile costs nj rounded up to a multiple of 4 rotation steps.
+      for (int done = 0; done < nj;) {
+        const int rem = nj - done;
+        const int gj = rem > 28 ? 32 : (rem > 12 ? 16 : (rem > 4 ? 8 : 4));
+        const int cnt = rem < gj ? rem : gj;
+        const int cl = lane & (gj - 1);
+        const int src = cl < cnt ? sIdx[warp][done + cl] : lane;
+        JRegs<COMBINE, ALCH> J;
+        {
+          const int js = 32 * jBlock + src;
+          const float4 xj = d.xyzq[js];
+          J.x = xj.x + shx;
+          J.y = xj.y + shy;
+          J.z = xj.z + shz;
+          J.q = xj.w;
+          const int tj = d.slotType[js];
+          J.meta = COMBINE ? src : ((src << 16) | tj);
+          if (COMBINE) {
+            const float2 lj2 = d.ljType[tj];
+            J.ex = lj2.x;
+            J.er = lj2.y;
+          }
+          if (ALCH && alchTile) {
+            J.b = d.slotSiteBlock[js];
+            J.l = J.b ? sLam[J.b & 0xFFFF] : 1.f;
+          }
+        }
+        if (cl >= cnt) J.x = 1.0e18f;  // empty compacted slot: never within rCut
+        J.fx = J.fy = J.fz = J.fl = 0.f;
+        const int rot = lane + 1;
+
+        if (!alchTile) {
+          if (masked)
+            plain_loop<ELEC, VDW, ENERGY, COMBINE, true>(J, xi, row, gj, rot, pc, sLJ, rowI, ljI, fix, fiy, fiz,
+                                                         ei, pairs, A.count);
+          else
+            plain_loop<ELEC, VDW, ENERGY, COMBINE, false>(J, xi, row, gj, rot, pc, sLJ, rowI, ljI, fix, fiy,
+                                                          fiz, ei, pairs, A.count);
+        } else if (ALCH) {
+          for (int k = 0; k < gj; k++) {
+            const float dx = xi.x - J.x, dy = xi.y - J.y, dz = xi.z - J.z;
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const int jb = COMBINE ? J.meta : (J.meta >> 16);
+            if (((row >> jb) & 1u) && r2 < pc.rc2) {
+              float c12, c6;
+              lj_params<COMBINE>(sLJ, rowI, J.meta & 0xFFFF, ljI, make_float2(J.ex, J.er), c12, c6);
+              const float rinv = rsqrt_approx(r2);
+              const float r = r2 * rinv;
+              const int bj = J.b;
+              const float lj = J.l;
+              // MSLD scaling, nbdirect.cu:244-254
+              const bool sameSite = (bi & 0xFFFF0000) == (bj & 0xFFFF0000);
+              const float s = sameSite ? (bi == bj ? li : 0.f) : li * lj;
+              const bool pert = (bi | bj) != 0;
+              float rEff = r, rinvE = rinv, r2E = r2, dredr = 1.f, dredll = 0.f;
+              if (ALCH == 2 && pert) {  // soft core, nbdirect.cu:257-275
+                const float rSoft = pc.softR * (1.f - s);
+                if (r < rSoft) {
+                  const float q = __fdividef(r, rSoft);
+                  const float f = fmaf(q * q * q, fmaf(-0.5f, q, 1.f), 0.5f);
+                  dredr = (3.f - 2.f * q) * q * q;
+                  dredll = -pc.softR * (f - dredr * q);
+                  rEff = f * rSoft;
+                  rinvE = rcp_approx(rEff);
+                  r2E = rEff * rEff;
+                }
+              }
+              float dEdr, E;
+              pair_terms<ELEC, VDW, true>(pc, rEff, r2E, rinvE, xi.w * J.q, c12, c6, dEdr, E);
+              dEdr *= s;
+              if (pert) {  // dU/dlambda routing, nbdirect.cu:400-415
+                const float fl = fmaf(dEdr, dredll, E);
+                if (sameSite) {
+                  if (bi == bj) fli += fl;
+                } else {
+                  fli = fmaf(lj, fl, fli);
+                  J.fl = fmaf(li, fl, J.fl);
+                }
+              }
+              const float fs = dEdr * dredr * rinv;
+              fix = fmaf(fs, dx, fix); fiy = fmaf(fs, dy, fiy); fiz = fmaf(fs, dz, fiz);
+              J.fx = fmaf(-fs, dx, J.fx); J.fy = fmaf(-fs, dy, J.fy); J.fz = fmaf(-fs, dz, J.fz);
+              if (ENERGY) ei += to_fix(s * E);
+              if (ENERGY && A.count) pairs++;
+            }
+            J.move(rot, gj);
+            J.move_forces(rot, gj, true);
+          }
+        }
+        // sum the group partials; group 0 lane p now holds compacted j done+p
+        float fx = J.fx, fy = J.fy, fz = J.fz, fl = J.fl;
+        for (int o = 16; o >= gj; o >>= 1) {
+          fx += __shfl_xor_sync(kFull, fx, o);
+          fy += __shfl_xor_sync(kFull, fy, o);
+          fz += __shfl_xor_sync(kFull, fz, o);
+          if (ALCH && alchTile) fl += __shfl_xor_sync(kFull, fl, o);
+        }
+        // deliver to the owner lane of each j atom of this chunk
+        const int from = (rank - done) & 31;
+        fx = __shfl_sync(kFull, fx, from);
+        fy = __shfl_sync(kFull, fy, from);
+        fz = __shfl_sync(kFull, fz, from);
+        if (ALCH && alchTile) fl = __shfl_sync(kFull, fl, from);
+        if (rank >= done && rank < done + cnt) {
+          ofx = fx; ofy = fy; ofz = fz; ofl = fl;
+        }
+        done += cnt;
       }
-      if (gj == 8) {
-        fx += __shfl_xor_sync(kFull, fx, 8); fy += __shfl_xor_sync(kFull, fy, 8);
-        fz += __shfl_xor_sync(kFull, fz, 8);
-        if (ALCH && alchTile) fl += __shfl_xor_sync(kFull, fl, 8);
+      __syncwarp();  // sIdx is rewritten by the next tile
+      if (jin && (ofx != 0.f || ofy != 0.f || ofz != 0.f)) {
+        red_add(&d.accF[jslot], to_fix(ofx));
+        red_add(&d.accF[S + jslot], to_fix(ofy));
+        red_add(&d.accF[2 * S + jslot], to_fix(ofz));
+        if (!(isfinite(ofx) && isfinite(ofy) && isfinite(ofz))) atomicOr(&d.ctr->status, kStatusNonFinite);
       }
-      // return to the owner lane of each surviving j atom
-      fx = __shfl_sync(kFull, fx, rank);
-      fy = __shfl_sync(kFull, fy, rank);
-      fz = __shfl_sync(kFull, fz, rank);
-      if (ALCH && alchTile) fl = __shfl_sync(kFull, fl, rank);
-      if (jin && (fx != 0.f || fy != 0.f || fz != 0.f)) {
-        red_add(&d.accF[jslot], to_fix(fx));
-        red_add(&d.accF[S + jslot], to_fix(fy));
-        red_add(&d.accF[2 * S + jslot], to_fix(fz));
-        if (!(isfinite(fx) && isfinite(fy) && isfinite(fz))) atomicOr(&d.ctr->status, kStatusNonFinite);
-      }
-      if (ALCH && alchTile && jin && bj0 && fl != 0.f)
+      if (ALCH && alchTile && jin && bj0 && ofl != 0.f)
         atomicAdd(reinterpret_cast<unsigned long long *>(&sAccL[bj0 & 0xFFFF]),
-                  static_cast<unsigned long long>(to_fix(fl)));
+                  static_cast<unsigned long long>(to_fix(ofl)));
     }
+    // the rest of the queue (< 64 entries) in chunks of 64, 32, 16 or 8,
+    // whichever pads least: e.g. 40 entries as 32 + 8 (20 steps, not 32)
+    for (int off = 0; off < nS;) {
+      const int rem = nS - off;
+      const int cap = rem > 48 ? 64 : (rem > 24 ? 32 : (rem > 12 ? 16 : 8));
+      const int cnt = rem < cap ? rem : cap;
+      stream_chunk<ELEC, VDW, ENERGY, COMBINE>(d, pc, sLJ, sStream[warp] + off, cnt, lane, xi, rowI, ljI, bx, by,
+                                               bz, fix2, fiy2, fiz2, ei, pairs, A.count);
+      off += cnt;
+    }
+    __syncwarp();  // sStream is rewritten by the next work item
+    fix += fix2.x + fix2.y;
+    fiy += fiy2.x + fiy2.y;
+    fiz += fiz2.x + fiz2.y;
     if (iValid && (fix != 0.f || fiy != 0.f || fiz != 0.f)) {
       red_add(&d.accF[islot], to_fix(fix));
       red_add(&d.accF[S + islot], to_fix(fiy));
@@ -781,6 +1058,7 @@ void launch_allpairs_ev(const AllPairsArgs &a, bool energy, dim3 grid, cudaStrea
 
 int launch_pair(const Dev &d, const PairConst &pc, const float *lambda, int elec, int vdw,
                 int alch, bool energy, bool count, int grid, cudaStream_t s) {
+  if (32LL * d.maxBlocks >= (1LL << 27)) return BNB_ERR_TOO_LARGE;  // streamed entries hold the slot in 27 bits
   KArgs a{d, pc, lambda, count ? 1 : 0};
   size_t shmem = d.ljCombine ? 0 : sizeof(float2) * d.nTypes * d.nTypes;
   shmem = (shmem + 15) & ~size_t(15);
