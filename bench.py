@@ -314,25 +314,52 @@ def run_bnb(args, rank, world):
         raise RuntimeError(f"device status {st} in timed region")
     t_total = sum(ms) / 1e3
 
-    # e2e: through the C ABI with host buffers, copies inside the timed region
+    # e2e: through the C ABI with host buffers, copies inside the timed
+    # regions.  Step k's region holds its pair work and, on a copy stream
+    # beside it, the H2D of frame k+1 and the D2H of step k-1's forces and
+    # energy (double-buffered); the region ends only when those copies are
+    # done.  Region 0 also holds the H2D of frame 0, the last region the D2H
+    # of the last step.  The outputs are overwritten (BNB_OUT_SET), so no
+    # clearing launch precedes a step.
     e2e = None
     if not args.no_e2e:
         host_frames = frames.cpu().pin_memory()
-        dpos = torch.empty(3 * s.N, dtype=torch.float32, device=dev)
-        hforce = torch.empty(3 * s.N, dtype=torch.float32).pin_memory()
-        henergy = torch.empty(1, dtype=torch.float64).pin_memory()
+        dpos = [torch.empty(3 * s.N, dtype=torch.float32, device=dev) for _ in range(2)]
+        dforce = [torch.empty(3 * s.N, dtype=torch.float32, device=dev) for _ in range(2)]
+        denergy = [torch.empty(1, dtype=torch.float64, device=dev) for _ in range(2)]
+        hforce = [torch.empty(3 * s.N, dtype=torch.float32).pin_memory() for _ in range(2)]
+        henergy = [torch.empty(1, dtype=torch.float64).pin_memory() for _ in range(2)]
+        copy = torch.cuda.Stream(device=dev)
         e_evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+        copied = [torch.cuda.Event() for _ in range(K)]
         nb.update_domdec(frames[W], True)
         torch.cuda.synchronize()
+        set_mode = _lib.BNB_OUT_SET
+
+        def e2e_step(k, pos, f, e):
+            if k % REBUILD_EVERY == 0:
+                nb.update_domdec(pos, True, asynchronous=(k > 0))
+            nb.getforce_nbdirect(pos, None, k % ENERGY_EVERY == 0, force=f, energy=e, mode=set_mode)
+
         for k in range(K):
             flush.zero_()
             e_evs[k][0].record(stream)
-            dpos.copy_(host_frames[W + k], non_blocking=True)
-            force.zero_()
-            energy.zero_()
-            step(k, dpos)
-            hforce.copy_(force, non_blocking=True)
-            henergy.copy_(energy, non_blocking=True)
+            copy.wait_stream(stream)
+            with torch.cuda.stream(copy):
+                if k == 0:
+                    dpos[0].copy_(host_frames[W], non_blocking=True)
+                    stream.wait_stream(copy)
+                if k + 1 < K:
+                    dpos[(k + 1) % 2].copy_(host_frames[W + k + 1], non_blocking=True)
+                if k > 0:
+                    hforce[(k - 1) % 2].copy_(dforce[(k - 1) % 2], non_blocking=True)
+                    henergy[(k - 1) % 2].copy_(denergy[(k - 1) % 2], non_blocking=True)
+                copied[k].record(copy)
+            e2e_step(k, dpos[k % 2], dforce[k % 2], denergy[k % 2])
+            stream.wait_event(copied[k])
+            if k == K - 1:
+                hforce[k % 2].copy_(dforce[k % 2], non_blocking=True)
+                henergy[k % 2].copy_(denergy[k % 2], non_blocking=True)
             e_evs[k][1].record(stream)
         torch.cuda.synchronize()
         t_e2e = sum(a.elapsed_time(b) for a, b in e_evs) / 1e3

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "libbnb.so")
 
 BNB_OK, BNB_ERR_ARG, BNB_ERR_CUDA, BNB_ERR_CAPACITY, BNB_ERR_UNSUPPORTED, BNB_ERR_STATE, BNB_ERR_DEVICE = range(7)
 BNB_ASYNC = 1
+BNB_OUT_SET, BNB_OUT_ADD64 = 2, 4   # output modes ORed into calcEnergy (include/bnb.h)
 STATUS_BLOCK_OVERFLOW, STATUS_TILE_OVERFLOW, STATUS_MASK_OVERFLOW, STATUS_WORK_OVERFLOW, STATUS_NONFINITE = 1, 2, 4, 8, 16
 _ERRORS = {1: "bad argument", 2: "CUDA error", 3: "list capacity exceeded", 4: "unsupported",
            5: "call order", 6: "device status", 7: "size above the fixed limit"}

@@ -19,7 +19,8 @@ the water bonds dropped.  With ``pme=True`` the electrostatics are complete:
 the 1-4 pairs and exclusion corrections (bnb_compute_nb14 / bnb_compute_nbex,
 lists from systems.with_pair_lists), PME reciprocal space and the Ewald self
 term (bnb_compute_pme / bnb_compute_ewald_self), as Potential::calc_force
-sums them (src/system/potential.cxx:1851-1941).  All replicas share one libbnb handle, so every kernel of a step
+sums them (src/system/potential.cxx:1851-1941); each adds into the step's FP64
+force and dU/dlambda (BNB_OUT_ADD64), so no per-term buffers or additions.  All replicas share one libbnb handle, so every kernel of a step
 covers all of them; ``capture`` records ``rebuild_every`` steps in one CUDA
 graph that is replayed.  Units are AKMA; dt is 2 fs.
 """
@@ -177,9 +178,6 @@ class MsldBatch:
         if pme:
             self.nb.set_pairs()
             self.nb.set_pme(order=pme_order)
-            self.f_term = torch.zeros(3 * N, dtype=f64, device=self.dev)   # per-term outputs, then added
-            self.l_term = torch.zeros(L, dtype=f64, device=self.dev)
-            self.e_term = torch.zeros(self.nb.R, dtype=f64, device=self.dev)
         self.nb.update_domdec(self.xf, True)               # synchronous first build sizes the list
         if tune:
             self.tuned_ms = self.autotune()
@@ -204,22 +202,15 @@ class MsldBatch:
         if self.bond_start is not None:
             _lib.call("bnb_bond_gradient", self.nb.N, _p(self.bond_start), _p(self.bond_partner),
                       _p(self.bond_param), _p(self.x), _p(self.force), s)
-        if self.pme:                                       # the other electrostatic terms of calc_force
-            for term in ("nb14", "nbex", "recip", "self"):
-                e = self.e_term if calc_e else None
-                if term == "recip":
-                    nb.getforce_ewald(self.xf, self.lamf, calc_e, force64=self.f_term, lambda_force64=self.l_term,
-                                      energy64=e, stream=stream)
-                elif term == "self":
-                    nb.getforce_ewaldself(self.lamf, calc_e, lambda_force64=self.l_term, energy64=e, stream=stream)
-                else:
-                    nb.getforce_pairs(term, self.xf, self.lamf, calc_e, force64=self.f_term,
-                                      lambda_force64=self.l_term, energy64=e, stream=stream)
-                if term != "self":
-                    self.force.add_(self.f_term)
-                self.lforce.add_(self.l_term)
-                if calc_e:
-                    self.energy.add_(self.e_term)
+        if self.pme:                                       # the other electrostatic terms of calc_force,
+            add = _lib.BNB_OUT_ADD64                       # each added into the step's FP64 outputs
+            e = self.energy if calc_e else None
+            for term in ("nb14", "nbex"):
+                nb.getforce_pairs(term, self.xf, self.lamf, calc_e, force64=self.force, lambda_force64=self.lforce,
+                                  energy64=e, stream=stream, mode=add)
+            nb.getforce_ewald(self.xf, self.lamf, calc_e, force64=self.force, lambda_force64=self.lforce,
+                              energy64=e, stream=stream, mode=add)
+            nb.getforce_ewaldself(self.lamf, calc_e, lambda_force64=self.lforce, energy64=e, stream=stream, mode=add)
         if self.fixed_bias is not None:
             _lib.call("bnb_bias", self.theta.numel(), _p(self.lam), _p(self.fixed_bias), self.n_var,
                       _p(self.var_bias), _p(self.lforce), None, s)

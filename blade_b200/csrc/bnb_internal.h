@@ -34,6 +34,20 @@ enum : int {
                        BNB_STATUS_MASK_OVERFLOW | BNB_STATUS_WORK_OVERFLOW,
 };
 
+// Output modes (BNB_OUT_SET / BNB_OUT_ADD64 of the public header).
+__device__ __forceinline__ void out64(double *p, double v, int mode) {
+  if (mode & BNB_OUT_ADD64) *p += v;
+  else *p = v;
+}
+__device__ __forceinline__ void out32(float *p, float v, int mode) {  // atomic unless overwriting
+  if (mode & BNB_OUT_SET) *p = v;
+  else if (v != 0.f) atomicAdd(p, v);
+}
+__device__ __forceinline__ void outE(double *p, double v, int mode) {
+  if (mode & BNB_OUT_SET) *p = v;
+  else *p += v;
+}
+
 struct RepInfo {          // per replica, device copy in Dev::rep
   float box[3];
   int atomStart, atomCount;

@@ -110,6 +110,11 @@ struct Arena {
 
 inline bool ok(cudaError_t e) { return e == cudaSuccess; }
 
+// calcEnergy of the compute calls: bit 0 the energy path, BNB_OUT_SET and
+// BNB_OUT_ADD64 the output modes; nothing else.
+inline bool flags_ok(int calcEnergy) { return (calcEnergy & ~(1 | BNB_OUT_SET | BNB_OUT_ADD64)) == 0; }
+inline int out_mode(int calcEnergy) { return calcEnergy & (BNB_OUT_SET | BNB_OUT_ADD64); }
+
 PairConst make_const(const bnb_params &p) {
   PairConst c{};
   double rc = p.rCut, rs = p.rSwitch, b = p.betaEwald;
@@ -651,7 +656,7 @@ int bnb_rebuild(bnb_handle *h, const float *position, const float *boxes, void *
 
 int bnb_compute(bnb_handle *h, const float *position, const float *lambda, const float *boxes,
                 int calcEnergy, const bnb_outputs *out, void *stream) {
-  if (!h || !out || !boxes || (h->N > 0 && !position)) return BNB_ERR_ARG;
+  if (!h || !out || !boxes || (h->N > 0 && !position) || !flags_ok(calcEnergy)) return BNB_ERR_ARG;
   if (!h->listBuilt) return BNB_ERR_STATE;
   if (h->alch && !lambda) return BNB_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
@@ -681,10 +686,10 @@ int bnb_compute(bnb_handle *h, const float *position, const float *lambda, const
   const bool rec = h->prof && h->pairN < kProfSlots;
   if (rec) cudaEventRecord(h->pairEv[2 * h->pairN], s);
   int rc = bnb::launch_pair(h->d, h->pc, lambda, h->p.elecMethod, h->p.vdwMethod, alch,
-                            calcEnergy != 0, h->counting, grid, s);
+                            (calcEnergy & 1) != 0, h->counting, grid, s);
   if (rec) cudaEventRecord(h->pairEv[2 * h->pairN++ + 1], s);
   if (rc) return rc;
-  bnb::launch_finalize(h->d, *out, s);
+  bnb::launch_finalize(h->d, *out, out_mode(calcEnergy), s);
   h->launches += 3;
   return ok(cudaGetLastError()) ? BNB_OK : BNB_ERR_CUDA;
 }
@@ -1060,19 +1065,20 @@ extern "C" int bnb_set_pairs(bnb_handle *h, int nb14Count, const bnb_nb14 *nb14,
 
 extern "C" int bnb_compute_nb14(bnb_handle *h, const float *position, const float *lambda, const float *boxes,
                                 int calcEnergy, const bnb_outputs *out, void *stream) {
-  if (!h || !out || !boxes || (h->N > 0 && !position)) return BNB_ERR_ARG;
+  if (!h || !out || !boxes || (h->N > 0 && !position) || !flags_ok(calcEnergy)) return BNB_ERR_ARG;
   if (!h->pairArena) return BNB_ERR_STATE;
   if (h->alch && !lambda) return BNB_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   int rc = pairs_boxes(h, boxes, s);
   if (rc) return rc;
   bnb::PairsArgs a = pairs_args(h, position, lambda);
-  return bnb::launch_nb14(a, *out, h->p.elecMethod, h->p.vdwMethod, h->soft14 && h->alch, calcEnergy != 0, s);
+  a.mode = out_mode(calcEnergy);
+  return bnb::launch_nb14(a, *out, h->p.elecMethod, h->p.vdwMethod, h->soft14 && h->alch, (calcEnergy & 1) != 0, s);
 }
 
 extern "C" int bnb_compute_nbex(bnb_handle *h, const float *position, const float *lambda, const float *boxes,
                                 int calcEnergy, const bnb_outputs *out, void *stream) {
-  if (!h || !out || !boxes || (h->N > 0 && !position)) return BNB_ERR_ARG;
+  if (!h || !out || !boxes || (h->N > 0 && !position) || !flags_ok(calcEnergy)) return BNB_ERR_ARG;
   if (!h->pairArena) return BNB_ERR_STATE;
   if (h->alch && !lambda) return BNB_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
@@ -1080,7 +1086,8 @@ extern "C" int bnb_compute_nbex(bnb_handle *h, const float *position, const floa
   if (rc) return rc;
   bnb::PairsArgs a = pairs_args(h, position, lambda);
   if (h->p.elecMethod != 1) a.nex = 0;  // the correction exists for PME only (pair.cu:379)
-  return bnb::launch_nbex(a, *out, calcEnergy != 0, s);
+  a.mode = out_mode(calcEnergy);
+  return bnb::launch_nbex(a, *out, (calcEnergy & 1) != 0, s);
 }
 
 
@@ -1256,7 +1263,7 @@ extern "C" int bnb_pme_grid(bnb_handle *h, int replica, int *K) {
 
 extern "C" int bnb_compute_pme(bnb_handle *h, const float *position, const float *lambda, const float *boxes,
                                int calcEnergy, const bnb_outputs *out, void *stream) {
-  if (!h || !out || !boxes || (h->N > 0 && !position)) return BNB_ERR_ARG;
+  if (!h || !out || !boxes || (h->N > 0 && !position) || !flags_ok(calcEnergy)) return BNB_ERR_ARG;
   if (!h->pmeOrder) return BNB_ERR_STATE;
   if (h->alch && !lambda) return BNB_ERR_ARG;
   if (h->p.elecMethod != 1) return BNB_OK;  // reciprocal space exists for PME only (nbrecip.cu:486)
@@ -1264,6 +1271,7 @@ extern "C" int bnb_compute_pme(bnb_handle *h, const float *position, const float
   int rc = pairs_boxes(h, boxes, s);
   if (rc) return rc;
   bnb::PmeArgs a = pme_args(h, position, lambda);
+  a.mode = out_mode(calcEnergy);
   if ((rc = bnb::pme_spread(a, s))) return rc;
   for (auto &p : h->pmePlans) {
     const bnb::PmeRep &f = h->pmeRep[p.first];
@@ -1281,16 +1289,17 @@ extern "C" int bnb_compute_pme(bnb_handle *h, const float *position, const float
       return BNB_ERR_CUDA;
   }
   h->launches += 4;
-  return bnb::pme_gather(a, *out, calcEnergy != 0, s);
+  return bnb::pme_gather(a, *out, (calcEnergy & 1) != 0, s);
 }
 
 extern "C" int bnb_compute_ewald_self(bnb_handle *h, const float *lambda, int calcEnergy, const bnb_outputs *out,
                                       void *stream) {
-  if (!h || !out) return BNB_ERR_ARG;
+  if (!h || !out || !flags_ok(calcEnergy)) return BNB_ERR_ARG;
   if (!h->pmeOrder) return BNB_ERR_STATE;
   if (h->alch && !lambda) return BNB_ERR_ARG;
   if (h->p.elecMethod != 1) return BNB_OK;  // nbrecip.cu:64
   bnb::PmeArgs a = pme_args(h, nullptr, lambda);
+  a.mode = out_mode(calcEnergy);
   h->launches += 1;
-  return bnb::pme_self(a, *out, calcEnergy != 0, (cudaStream_t)stream);
+  return bnb::pme_self(a, *out, (calcEnergy & 1) != 0, (cudaStream_t)stream);
 }

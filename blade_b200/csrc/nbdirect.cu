@@ -858,7 +858,7 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
 // One thread per atom, in atom order: the outputs (in the caller's atom
 // order) are written coalesced, and the per-slot accumulators, still in L2
 // from the pair kernel's atomics, are gathered through atomSlot.
-__global__ void k_finalize(Dev d, bnb_outputs o) {
+__global__ void k_finalize(Dev d, bnb_outputs o, int mode) {
   const int S = 32 * d.maxBlocks;
   const double inv = 1.0 / kFixScale;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < d.N; a += gridDim.x * blockDim.x) {
@@ -868,8 +868,8 @@ __global__ void k_finalize(Dev d, bnb_outputs o) {
       const long long v = d.accF[k * S + t];
       if (v) d.accF[k * S + t] = 0;
       const double f = (double)v * inv;
-      if (o.force64) o.force64[3 * a + k] = f;
-      if (o.force && v) atomicAdd(&o.force[3 * a + k], (float)f);
+      if (o.force64) out64(&o.force64[3 * a + k], f, mode);
+      if (o.force) out32(&o.force[3 * a + k], (float)f, mode);
     }
   }
   if (blockIdx.x == 0) {
@@ -878,15 +878,15 @@ __global__ void k_finalize(Dev d, bnb_outputs o) {
       long long v = d.accL[i];
       d.accL[i] = 0;
       double f = (double)v * inv;
-      if (o.lambdaForce64) o.lambdaForce64[i] = f;
-      if (o.lambdaForce && v) atomicAdd(&o.lambdaForce[i], (float)f);
+      if (o.lambdaForce64) out64(&o.lambdaForce64[i], f, mode);
+      if (o.lambdaForce) out32(&o.lambdaForce[i], (float)f, mode);
     }
     for (int r = threadIdx.x; r < d.R; r += blockDim.x) {
       long long v = d.accE[r];
       d.accE[r] = 0;
       double e = (double)v * inv;
-      if (o.energy64) o.energy64[r] = e;
-      if (o.energy) o.energy[r] += e;
+      if (o.energy64) out64(&o.energy64[r], e, mode);
+      if (o.energy) outE(&o.energy[r], e, mode);
     }
   }
 }
@@ -1079,12 +1079,12 @@ int launch_pair(const Dev &d, const PairConst &pc, const float *lambda, int elec
   return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
 }
 
-void launch_finalize(const Dev &d, const bnb_outputs &o, cudaStream_t s) {
+void launch_finalize(const Dev &d, const bnb_outputs &o, int mode, cudaStream_t s) {
   int n = d.N;
   int grid = (n + 255) / 256;
   if (grid > 148 * 8) grid = 148 * 8;
   if (grid < 1) grid = 1;
-  k_finalize<<<grid, 256, 0, s>>>(d, o);
+  k_finalize<<<grid, 256, 0, s>>>(d, o, mode);
 }
 
 int launch_allpairs(const AllPairsArgs &a, const bnb_outputs &o, int elec, int vdw, bool energy,

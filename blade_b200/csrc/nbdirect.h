@@ -8,7 +8,7 @@ namespace bnb {
 // alch: 0 none, 1 MSLD scaling, 2 MSLD + soft core.
 int launch_pair(const Dev &d, const PairConst &pc, const float *lambda, int elec, int vdw,
                 int alch, bool energy, bool count, int grid, cudaStream_t s);
-void launch_finalize(const Dev &d, const bnb_outputs &o, cudaStream_t s);
+void launch_finalize(const Dev &d, const bnb_outputs &o, int mode, cudaStream_t s);
 
 // All-pairs evaluation of one small system (bnb_nbdirect_noalloc).  accF is
 // [3 * stride] (component planes), accE one entry; both must be zero on

@@ -174,23 +174,23 @@ __global__ void k_pairs_finalize(PairsArgs a, bnb_outputs o) {
     const long long v = a.accF[t];
     if (v) a.accF[t] = 0;
     const double f = (double)v * inv;
-    if (o.force64) o.force64[t] = f;
-    if (o.force && v) atomicAdd(&o.force[t], (float)f);
+    if (o.force64) out64(&o.force64[t], f, a.mode);
+    if (o.force) out32(&o.force[t], (float)f, a.mode);
   }
   if (blockIdx.x == 0) {
     for (int i = threadIdx.x; i < a.lamTotal; i += blockDim.x) {
       const long long v = a.accL[i];
       a.accL[i] = 0;
       const double f = (double)v * inv;
-      if (o.lambdaForce64) o.lambdaForce64[i] = f;
-      if (o.lambdaForce && v) atomicAdd(&o.lambdaForce[i], (float)f);
+      if (o.lambdaForce64) out64(&o.lambdaForce64[i], f, a.mode);
+      if (o.lambdaForce) out32(&o.lambdaForce[i], (float)f, a.mode);
     }
     for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
       const long long v = a.accE[r];
       a.accE[r] = 0;
       const double e = (double)v * inv;
-      if (o.energy64) o.energy64[r] = e;
-      if (o.energy) o.energy[r] += e;
+      if (o.energy64) out64(&o.energy64[r], e, a.mode);
+      if (o.energy) outE(&o.energy[r], e, a.mode);
     }
   }
 }

@@ -18,6 +18,7 @@ struct PairsArgs {
   long long *accF;           // [3N] fixed-point dU/dx, atom order
   long long *accL;           // [lamTotal]
   long long *accE;           // [R]
+  int mode;                  // BNB_OUT_SET / BNB_OUT_ADD64 bits of the call
 };
 int launch_nb14(const PairsArgs &a, const bnb_outputs &o, int elec, int vdw, bool soft, bool energy,
                 cudaStream_t s);

@@ -179,16 +179,16 @@ __device__ void finalize_outputs(const PmeArgs &a, const bnb_outputs &o, bool en
     const long long v = __ldcg(&a.accL[i]);
     a.accL[i] = 0;
     const double f = (double)v * inv;
-    if (o.lambdaForce64) o.lambdaForce64[i] = f;
-    if (o.lambdaForce && v) atomicAdd(&o.lambdaForce[i], (float)f);
+    if (o.lambdaForce64) out64(&o.lambdaForce64[i], f, a.mode);
+    if (o.lambdaForce) out32(&o.lambdaForce[i], (float)f, a.mode);
   }
   if (energy)
     for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
       const long long v = __ldcg(&a.accE[r]);
       a.accE[r] = 0;
       const double e = (double)v * inv;
-      if (o.energy64) o.energy64[r] = e;
-      if (o.energy) o.energy[r] += e;
+      if (o.energy64) out64(&o.energy64[r], e, a.mode);
+      if (o.energy) outE(&o.energy[r], e, a.mode);
     }
 }
 
@@ -283,14 +283,14 @@ __global__ void __launch_bounds__(256) k_gather(PmeArgs a, bnb_outputs o) {
     const float fy = c * gy * ((float)pr.K[1] / ri.box[1]);
     const float fz = c * gz * ((float)pr.K[2] / ri.box[2]);
     if (o.force64) {
-      o.force64[3 * atom] = fx;
-      o.force64[3 * atom + 1] = fy;
-      o.force64[3 * atom + 2] = fz;
+      out64(&o.force64[3 * atom], fx, a.mode);
+      out64(&o.force64[3 * atom + 1], fy, a.mode);
+      out64(&o.force64[3 * atom + 2], fz, a.mode);
     }
     if (o.force) {
-      atomicAdd(&o.force[3 * atom], fx);
-      atomicAdd(&o.force[3 * atom + 1], fy);
-      atomicAdd(&o.force[3 * atom + 2], fz);
+      out32(&o.force[3 * atom], fx, a.mode);
+      out32(&o.force[3 * atom + 1], fy, a.mode);
+      out32(&o.force[3 * atom + 2], fz, a.mode);
     }
     if (block) red_add(&a.accL[block], to_fix(2.f * qraw * phi));
     if (ENERGY) e = qe * phi;

@@ -33,6 +33,7 @@ struct PmeArgs {
   long long *accL;         // [lamTotal]
   long long *accE;         // [R]
   unsigned int *done;      // CTAs finished in the current gather / self launch (zero between launches)
+  int mode;                // BNB_OUT_SET / BNB_OUT_ADD64 bits of the call
 };
 
 // Spread lambda-scaled charges into qfix and convert to the FP32 grid

@@ -110,12 +110,13 @@ class NbDirect:
 
     def getforce_nbdirect(self, positions, lambdas=None, calc_energy=True, force=None,
                           lambda_force=None, energy=None, force64=None, lambda_force64=None,
-                          energy64=None, stream=None, boxes=None):
+                          energy64=None, stream=None, boxes=None, mode=0):
+        """bnb_compute; ``mode`` ORs in BNB_OUT_SET / BNB_OUT_ADD64 (output modes)."""
         out = _lib.Outputs(force=_ptr(force), lambdaForce=_ptr(lambda_force), energy=_ptr(energy),
                            force64=_ptr(force64), lambdaForce64=_ptr(lambda_force64), energy64=_ptr(energy64))
         b = np.ascontiguousarray(self.boxes if boxes is None else boxes, np.float32)
         _lib.call("bnb_compute", self.h, _ptr(positions), _ptr(lambdas), b.ctypes.data_as(C.c_void_p),
-                  int(bool(calc_energy)), C.byref(out), _stream(stream))
+                  int(bool(calc_energy)) | int(mode), C.byref(out), _stream(stream))
 
     # -- nb14 / nbex pair lists (getforce_nb14 / getforce_nbex) ---------------------
     def set_pairs(self, soft14: bool = False):
@@ -139,13 +140,13 @@ class NbDirect:
 
     def getforce_pairs(self, which: str, positions, lambdas=None, calc_energy=True, force=None,
                        lambda_force=None, energy=None, force64=None, lambda_force64=None, energy64=None,
-                       stream=None, boxes=None):
+                       stream=None, boxes=None, mode=0):
         """bnb_compute_nb14 (which="nb14") or bnb_compute_nbex (which="nbex")."""
         out = _lib.Outputs(force=_ptr(force), lambdaForce=_ptr(lambda_force), energy=_ptr(energy),
                            force64=_ptr(force64), lambdaForce64=_ptr(lambda_force64), energy64=_ptr(energy64))
         b = np.ascontiguousarray(self.boxes if boxes is None else boxes, np.float32)
         _lib.call("bnb_compute_" + which, self.h, _ptr(positions), _ptr(lambdas), b.ctypes.data_as(C.c_void_p),
-                  int(bool(calc_energy)), C.byref(out), _stream(stream))
+                  int(bool(calc_energy)) | int(mode), C.byref(out), _stream(stream))
 
     def evaluate_pairs(self, which: str, positions=None, lambdas=None, calc_energy=True):
         import torch
@@ -173,20 +174,21 @@ class NbDirect:
         return tuple(int(k) for k in K)
 
     def getforce_ewald(self, positions, lambdas=None, calc_energy=True, force=None, lambda_force=None,
-                       energy=None, force64=None, lambda_force64=None, energy64=None, stream=None, boxes=None):
+                       energy=None, force64=None, lambda_force64=None, energy64=None, stream=None, boxes=None,
+                       mode=0):
         """bnb_compute_pme (getforce_ewald)."""
         out = _lib.Outputs(force=_ptr(force), lambdaForce=_ptr(lambda_force), energy=_ptr(energy),
                            force64=_ptr(force64), lambdaForce64=_ptr(lambda_force64), energy64=_ptr(energy64))
         b = np.ascontiguousarray(self.boxes if boxes is None else boxes, np.float32)
         _lib.call("bnb_compute_pme", self.h, _ptr(positions), _ptr(lambdas), b.ctypes.data_as(C.c_void_p),
-                  int(bool(calc_energy)), C.byref(out), _stream(stream))
+                  int(bool(calc_energy)) | int(mode), C.byref(out), _stream(stream))
 
     def getforce_ewaldself(self, lambdas=None, calc_energy=True, lambda_force=None, energy=None,
-                           lambda_force64=None, energy64=None, stream=None):
+                           lambda_force64=None, energy64=None, stream=None, mode=0):
         """bnb_compute_ewald_self (getforce_ewaldself)."""
         out = _lib.Outputs(lambdaForce=_ptr(lambda_force), energy=_ptr(energy), lambdaForce64=_ptr(lambda_force64),
                            energy64=_ptr(energy64))
-        _lib.call("bnb_compute_ewald_self", self.h, _ptr(lambdas), int(bool(calc_energy)), C.byref(out),
+        _lib.call("bnb_compute_ewald_self", self.h, _ptr(lambdas), int(bool(calc_energy)) | int(mode), C.byref(out),
                   _stream(stream))
 
     def evaluate_pme(self, positions=None, lambdas=None, calc_energy=True):

@@ -136,6 +136,18 @@ typedef struct {
   double *lambdaForce64;
   double *energy64;
 } bnb_outputs;
+/*
+ * Output modes, ORed into calcEnergy (whose bit 0 alone selects the energy
+ * path) of bnb_compute, bnb_compute_nb14/nbex, bnb_compute_pme and
+ * bnb_compute_ewald_self.  No reference counterpart; they save the caller a
+ * clearing launch (BNB_OUT_SET: force, lambdaForce and energy are written
+ * rather than added to -- on a force-only call energy receives 0) or an
+ * addition per term (BNB_OUT_ADD64: force64, lambdaForce64 and energy64 are
+ * added to rather than written; calls that add into one array must be ordered
+ * on one stream).
+ */
+#define BNB_OUT_SET 2
+#define BNB_OUT_ADD64 4
 int bnb_compute(bnb_handle *h, const float *position, const float *lambda,
                 const float *boxes, int calcEnergy, const bnb_outputs *out,
                 void *stream);

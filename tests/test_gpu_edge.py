@@ -152,3 +152,34 @@ def test_msld_lambda_kernels(cuda):
     olf, oe = oracle.bias(ol, fb, vb)
     np.testing.assert_allclose(lf.cpu().numpy(), olf, rtol=1e-5, atol=1e-6)
     assert float(en[0]) == pytest.approx(oe, rel=1e-6)
+
+
+def test_output_modes(cuda):
+    """BNB_OUT_SET overwrites force / lambdaForce / energy; BNB_OUT_ADD64 adds
+    into force64 / lambdaForce64 / energy64; the default adds and overwrites."""
+    from blade_b200 import _lib
+    s = systems.msld_water()
+    nb = NbDirect(s)
+    pos, lam = nb.positions_tensor(), nb.lambdas_tensor()
+    nb.update_domdec(pos, True)
+    f64, l64, e64 = nb.evaluate(pos, lam)
+    N3, L = 3 * s.N, nb.L
+    f = torch.full((N3,), 7.0, device="cuda")
+    lf = torch.full((L,), -3.0, device="cuda")
+    e = torch.full((1,), 11.0, dtype=torch.float64, device="cuda")
+    nb.getforce_nbdirect(pos, lam, True, force=f, lambda_force=lf, energy=e, mode=_lib.BNB_OUT_SET)
+    torch.cuda.synchronize()
+    assert torch.allclose(f.double(), f64.reshape(-1), rtol=1e-6, atol=1e-5)
+    assert torch.allclose(lf.double(), l64, rtol=1e-6, atol=1e-5)
+    assert float(e[0]) == float(e64[0])
+    g = torch.full((N3,), 2.5, dtype=torch.float64, device="cuda")
+    gl = torch.full((L,), 1.5, dtype=torch.float64, device="cuda")
+    ge = torch.full((1,), -4.0, dtype=torch.float64, device="cuda")
+    nb.getforce_nbdirect(pos, lam, True, force64=g, lambda_force64=gl, energy64=ge, mode=_lib.BNB_OUT_ADD64)
+    torch.cuda.synchronize()
+    assert torch.equal(g, 2.5 + f64.reshape(-1))
+    assert torch.equal(gl, 1.5 + l64)
+    assert float(ge[0]) == -4.0 + float(e64[0])
+    with pytest.raises(_lib.BnbError):
+        nb.getforce_nbdirect(pos, lam, True, force64=g, mode=8)
+    nb.close()
