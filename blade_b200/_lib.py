@@ -98,6 +98,7 @@ def lib():
             "bnb_bond_gradient": (i, [i, p, p, p, p, p, p]),
             "bnb_langevin_vrorv": (i, [i, i, p, p, p, p, p, p, p, p, d, d, d, d, d, C.c_ulonglong, C.c_ulonglong,
                                        p, p, p, p]),
+            "bnb_set_box_type": (i, [p, i]),
             "bnb_version": (C.c_char_p, []),
         }
         for name, (res, args) in sig.items():

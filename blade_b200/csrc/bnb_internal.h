@@ -48,14 +48,43 @@ __device__ __forceinline__ void outE(double *p, double v, int mode) {
   else *p += v;
 }
 
+// Box of a replica.  A = (box[0], 0, 0), B = (tric[0], box[1], 0),
+// C = (tric[1], tric[2], box[2]): the lower-triangular cell of the
+// reference's State::tricBox (src/system/state.h); tric is zero for an
+// orthorhombic box.  Atoms are wrapped into the brick [0,A)x[0,B_y)x[0,C_z),
+// a fundamental domain of that lattice (src/main/real3.h:340-360).
+// shift[code] = sx A + sy B + sz C for the 14 half-shell images.
 struct RepInfo {          // per replica, device copy in Dev::rep
   float box[3];
   int atomStart, atomCount;
   int colStart, nCols;
   int divX, divY;
   int lamStart, lamCount;
-  int pad;
+  float tric[3];          // B_x, C_x, C_y
+  float4 shift[14];       // image shift vectors by shift code (kNumShifts)
 };
+
+// Lattice translation sx A + sy B + sz C in FP32, one rounding per operation
+// in a fixed order (the reference's xj.x += shift.z*C_x + shift.y*B_x +
+// shift.x*A_x, src/nbdirect/nbdirect.cu:196-199).
+__host__ __device__ __forceinline__ float3 lattice_shift(const float *box, const float *tric, int sx, int sy,
+                                                         int sz) {
+  const float fx = (float)sx, fy = (float)sy, fz = (float)sz;
+  float3 v;
+#ifdef __CUDA_ARCH__
+  v.x = __fadd_rn(__fadd_rn(__fmul_rn(fz, tric[1]), __fmul_rn(fy, tric[0])), __fmul_rn(fx, box[0]));
+  v.y = __fadd_rn(__fmul_rn(fz, tric[2]), __fmul_rn(fy, box[1]));
+  v.z = __fmul_rn(fz, box[2]);
+#else
+  volatile float t0 = fz * tric[1], t1 = fy * tric[0], t2 = fx * box[0];
+  volatile float s0 = t0 + t1;
+  v.x = s0 + t2;
+  volatile float u0 = fz * tric[2], u1 = fy * box[1];
+  v.y = u0 + u1;
+  v.z = fz * box[2];
+#endif
+  return v;
+}
 
 // Device-side scalar counters written by the list builder.
 struct Counters {

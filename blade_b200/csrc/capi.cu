@@ -33,6 +33,7 @@ using bnb::RepInfo;
 struct bnb_handle {
   bnb_params p;
   int R = 0, N = 0;
+  int triclinic = 0;  // boxes arrays: 3 floats per replica, or 6 (State::tricBox_f layout)
   std::vector<int> atomCount, atomStart;
   // topology
   bool topo = false;
@@ -258,6 +259,65 @@ int alloc_list(bnb_handle *h) {
   return BNB_OK;
 }
 
+// Box of replica r from a caller's boxes array: three edge lengths, or after
+// bnb_set_box_type(h, 1) six floats in the layout of State::tricBox_f
+// (A_x, B_x, B_y, C_x, C_y, C_z; src/system/state.h).
+void box_of(const bnb_handle *h, const float *boxes, int r, float b[3], float t[3]) {
+  if (h->triclinic) {
+    const float *q = boxes + 6 * r;
+    b[0] = q[0]; b[1] = q[2]; b[2] = q[5];
+    t[0] = q[1]; t[1] = q[3]; t[2] = q[4];
+  } else {
+    for (int k = 0; k < 3; k++) { b[k] = boxes[3 * r + k]; t[k] = 0.f; }
+  }
+}
+
+// Image shift vectors of the 14 half-shell codes for a replica's box.  The
+// integer shifts follow the reference's cull over neighbouring domains for a
+// single domain (src/domdec/cull.cu:141-190): z in {0,1}; y in y0 + {-z..1}
+// with y0 = -floor(z C_y / B_y + 1/2); x in x0 + {-(y'!=0||z!=0)..1} with
+// x0 = -floor((z C_x + y B_x) / A_x + 1/2), y' the uncentred y.  For an
+// orthorhombic box y0 = x0 = 0 and the codes are the plain half shell.
+void set_shifts(RepInfo &ri) {
+  for (int code = 0; code < bnb::kNumShifts; code++) {
+    int x, y, z;
+    if (code < 2) { x = code; y = 0; z = 0; }
+    else if (code < 5) { x = code - 3; y = 1; z = 0; }
+    else { int c = code - 5; x = c % 3 - 1; y = c / 3 - 1; z = 1; }
+    // one rounding per operation (no contraction), as the CPU restatement
+    volatile float ty = (float)z * ri.tric[2];
+    volatile float qy = ty / ri.box[1];
+    const int y0 = -(int)std::floor(qy + 0.5f);
+    const int sy = y + y0;
+    volatile float tx0 = (float)z * ri.tric[1], tx1 = (float)sy * ri.tric[0];
+    volatile float sxy = tx0 + tx1;
+    volatile float qx = sxy / ri.box[0];
+    const int x0 = -(int)std::floor(qx + 0.5f);
+    const int sx = x + x0;
+    const float3 v = bnb::lattice_shift(ri.box, ri.tric, sx, sy, z);
+    ri.shift[code] = make_float4(v.x, v.y, v.z, 0.f);
+  }
+}
+
+// Stores the boxes of all replicas; returns true if any changed.
+bool store_boxes(bnb_handle *h, const float *boxes) {
+  bool changed = false;
+  for (int r = 0; r < h->R; r++) {
+    float b[3], t[3];
+    box_of(h, boxes, r, b, t);
+    RepInfo &ri = h->rep[r];
+    bool c = false;
+    for (int k = 0; k < 3; k++)
+      if (ri.box[k] != b[k] || ri.tric[k] != t[k]) c = true;
+    if (c) {
+      for (int k = 0; k < 3; k++) { ri.box[k] = b[k]; ri.tric[k] = t[k]; }
+      set_shifts(ri);
+      changed = true;
+    }
+  }
+  return changed;
+}
+
 // Column grid per replica from its box; returns true if the layout changed.
 bool layout_columns(bnb_handle *h, const float *boxes) {
   bool changed = false;
@@ -266,18 +326,20 @@ bool layout_columns(bnb_handle *h, const float *boxes) {
   for (int r = 0; r < h->R; r++) {
     RepInfo &ri = h->rep[r];
     int dx, dy;
-    bnb_domain_div(h->atomCount[r], boxes + 3 * r, &dx, &dy);
+    float b[3], t[3];
+    box_of(h, boxes, r, b, t);
+    bnb_domain_div(h->atomCount[r], b, &dx, &dy);
     if (dx != ri.divX || dy != ri.divY || col != ri.colStart) changed = true;
     ri.divX = dx;
     ri.divY = dy;
     ri.colStart = col;
     ri.nCols = dx * dy;
-    for (int k = 0; k < 3; k++) ri.box[k] = boxes[3 * r + k];
     for (int c = 0; c < ri.nCols; c++) colRep.push_back(r);
     col += ri.nCols;
   }
   h->totalCols = col;
   h->colRep.swap(colRep);
+  store_boxes(h, boxes);
   return changed;
 }
 
@@ -338,6 +400,16 @@ void bnb_default_params(bnb_params *p) {
 }
 
 const char *bnb_version(void) { return "bnb 0.1 (sm_100a)"; }
+
+int bnb_set_box_type(bnb_handle *h, int triclinic) {
+  if (!h || (triclinic != 0 && triclinic != 1)) return BNB_ERR_ARG;
+  if (triclinic && h->pmeOrder) return BNB_ERR_UNSUPPORTED;  // PME grids are orthorhombic here
+  if (h->triclinic != triclinic) {
+    h->triclinic = triclinic;
+    h->listBuilt = false;  // the next rebuild reads the boxes in the new layout
+  }
+  return BNB_OK;
+}
 
 int bnb_domain_div(int atomCount, const float *box, int *divX, int *divY) {
   if (!box || !divX || !divY || atomCount < 0) return BNB_ERR_ARG;
@@ -563,11 +635,12 @@ int bnb_set_topology(bnb_handle *h, const bnb_nbond *nbonds, const int *typeCoun
 int bnb_rebuild(bnb_handle *h, const float *position, const float *boxes, void *stream, int flags) {
   if (!h || !boxes || (h->N > 0 && !position)) return BNB_ERR_ARG;
   if (!h->topo) return BNB_ERR_STATE;
-  for (int r = 0; r < h->R; r++)
-    for (int k = 0; k < 3; k++) {
-      float L = boxes[3 * r + k];
-      if (!(L >= 2 * h->p.rCut)) return BNB_ERR_ARG;  // single-image scheme needs rCut <= box/2
-    }
+  for (int r = 0; r < h->R; r++) {
+    float b[3], t[3];
+    box_of(h, boxes, r, b, t);
+    for (int k = 0; k < 3; k++)  // single-image scheme needs rCut <= half of every brick edge
+      if (!(b[k] >= 2 * h->p.rCut) || !std::isfinite(t[k])) return BNB_ERR_ARG;
+  }
   cudaStream_t s = (cudaStream_t)stream;
   const bool async = (flags & BNB_ASYNC) != 0;
   bool changed = layout_columns(h, boxes);
@@ -660,13 +733,7 @@ int bnb_compute(bnb_handle *h, const float *position, const float *lambda, const
   if (!h->listBuilt) return BNB_ERR_STATE;
   if (h->alch && !lambda) return BNB_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
-  bool boxChanged = false;
-  for (int r = 0; r < h->R; r++)
-    for (int k = 0; k < 3; k++)
-      if (h->rep[r].box[k] != boxes[3 * r + k]) {
-        h->rep[r].box[k] = boxes[3 * r + k];
-        boxChanged = true;
-      }
+  const bool boxChanged = store_boxes(h, boxes);
   if (boxChanged) {
     int rc = upload_rep(h, s);
     if (rc) return rc;
@@ -984,14 +1051,7 @@ extern "C" int bnb_nbdirect_noalloc(const bnb_params *p, int atomCount, const fl
 // ---------------------------------------------------------------------------
 namespace {
 int pairs_boxes(bnb_handle *h, const float *boxes, cudaStream_t s) {
-  bool changed = false;
-  for (int r = 0; r < h->R; r++)
-    for (int k = 0; k < 3; k++)
-      if (h->rep[r].box[k] != boxes[3 * r + k]) {
-        h->rep[r].box[k] = boxes[3 * r + k];
-        changed = true;
-      }
-  return changed ? upload_rep(h, s) : BNB_OK;
+  return store_boxes(h, boxes) ? upload_rep(h, s) : BNB_OK;
 }
 
 bnb::PairsArgs pairs_args(bnb_handle *h, const float *position, const float *lambda) {
@@ -1162,6 +1222,7 @@ bnb::PmeArgs pme_args(bnb_handle *h, const float *position, const float *lambda)
 }  // namespace
 
 extern "C" int bnb_set_pme(bnb_handle *h, int order, float gridSpace, const int *grid, const float *boxes) {
+  if (h && h->triclinic) return BNB_ERR_UNSUPPORTED;  // PME grids are orthorhombic here
   if (!h || !boxes || (order != 4 && order != 6 && order != 8) || (!grid && !(gridSpace > 0.f)))
     return BNB_ERR_ARG;
   if (!h->topo) return BNB_ERR_STATE;

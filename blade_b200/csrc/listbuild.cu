@@ -31,17 +31,7 @@ __device__ __forceinline__ uint32_t z_key(float z) {
   return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
-__device__ __forceinline__ int shift_code_vec(int code, int *sx, int *sy) {
-  // Half shell of cull.cu:127-173: z in {0,1}; y in {-z..1};
-  // x in {-(y!=0||z!=0)..1}.  Codes enumerate that loop in order.
-  // code: 0,1 -> (0..1,0,0); 2..4 -> (-1..1,1,0); 5..13 -> (-1..1,-1..1,1)
-  int x, y, z;
-  if (code < 2) { x = code; y = 0; z = 0; }
-  else if (code < 5) { x = code - 3; y = 1; z = 0; }
-  else { int c = code - 5; x = c % 3 - 1; y = c / 3 - 1; z = 1; }
-  *sx = x; *sy = y;
-  return z;
-}
+
 
 // AABB gap^2 <= c2 with the operation order of orc_aabb_hit.
 __device__ __forceinline__ bool aabb_hit(float4 imin, float4 imax, float4 jmin,
@@ -202,19 +192,25 @@ __global__ void k_bin(Dev d, const float *__restrict__ pos) {
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a == 0) atomicAnd(&d.ctr->status, ~kStatusListInvalid);  // this rebuild starts a fresh list
   if (a >= d.N) return;
-  const RepInfo ri = d.rep[d.atomRep[a]];
-  float w[3];
-  int s[3];
-#pragma unroll
-  for (int k = 0; k < 3; k++) {
-    float x = pos[3 * a + k];
-    if (!isfinite(x)) atomicOr(&d.ctr->status, kStatusNonFinite);
-    float L = ri.box[k];
-    float f = floorf(__fdiv_rn(x, L));
-    f = fminf(fmaxf(f, -127.0f), 127.0f);
-    s[k] = (int)f;
-    w[k] = __fsub_rn(x, __fmul_rn(f, L));
-  }
+  const RepInfo &ri = d.rep[d.atomRep[a]];
+  const float x = pos[3 * a], y = pos[3 * a + 1], z = pos[3 * a + 2];
+  if (!(isfinite(x) && isfinite(y) && isfinite(z))) atomicOr(&d.ctr->status, kStatusNonFinite);
+  // Image shift as the reference's triclinic modulus (src/main/real3.h:340-360):
+  // z by C, then y by B, then x by A; for an orthorhombic box the three are
+  // independent.
+  float fz = floorf(__fdiv_rn(z, ri.box[2]));
+  fz = fminf(fmaxf(fz, -127.0f), 127.0f);
+  const float yz = __fsub_rn(y, __fmul_rn(fz, ri.tric[2]));
+  const float xz = __fsub_rn(x, __fmul_rn(fz, ri.tric[1]));
+  float fy = floorf(__fdiv_rn(yz, ri.box[1]));
+  fy = fminf(fmaxf(fy, -127.0f), 127.0f);
+  const float xy = __fsub_rn(xz, __fmul_rn(fy, ri.tric[0]));
+  float fx = floorf(__fdiv_rn(xy, ri.box[0]));
+  fx = fminf(fmaxf(fx, -127.0f), 127.0f);
+  int s[3] = {(int)fx, (int)fy, (int)fz};
+  // the packed (wrapped) coordinates, as k_pack computes them
+  const float3 L = lattice_shift(ri.box, ri.tric, s[0], s[1], s[2]);
+  float w[3] = {__fsub_rn(x, L.x), __fsub_rn(y, L.y), __fsub_rn(z, L.z)};
   d.wrap[a] = (s[0] + 128) | ((s[1] + 128) << 8) | ((s[2] + 128) << 16);
   int ix = (int)floorf(__fmul_rn(__fdiv_rn(w[0], ri.box[0]), (float)ri.divX));
   ix = ix >= ri.divX ? ri.divX - 1 : ix;
@@ -410,11 +406,11 @@ __global__ void k_pack(Dev d, const float *__restrict__ pos, bool columns) {
   float3 mx = make_float3(-INFINITY, -INFINITY, -INFINITY);
   if (a >= 0) {
     int w = d.wrap[a];
-    float sx = (float)((w & 0xFF) - 128), sy = (float)(((w >> 8) & 0xFF) - 128),
-          sz = (float)(((w >> 16) & 0xFF) - 128);
-    p.x = __fsub_rn(pos[3 * a], __fmul_rn(sx, ri.box[0]));
-    p.y = __fsub_rn(pos[3 * a + 1], __fmul_rn(sy, ri.box[1]));
-    p.z = __fsub_rn(pos[3 * a + 2], __fmul_rn(sz, ri.box[2]));
+    const float3 L = lattice_shift(ri.box, ri.tric, (w & 0xFF) - 128, ((w >> 8) & 0xFF) - 128,
+                                   ((w >> 16) & 0xFF) - 128);
+    p.x = __fsub_rn(pos[3 * a], L.x);
+    p.y = __fsub_rn(pos[3 * a + 1], L.y);
+    p.z = __fsub_rn(pos[3 * a + 2], L.z);
     mn = p;
     mx = p;
   }
@@ -470,9 +466,8 @@ __global__ void k_cull(Dev d, float rcull2) {
     }
     int r = d.blockRep[iBlock];
     const RepInfo &ri = d.rep[r];
-    int sx, sy, sz = shift_code_vec(code, &sx, &sy);
-    float3 sh = make_float3(__fmul_rn((float)sx, ri.box[0]), __fmul_rn((float)sy, ri.box[1]),
-                            __fmul_rn((float)sz, ri.box[2]));
+    const float4 sv = ri.shift[code];
+    const float3 sh = make_float3(sv.x, sv.y, sv.z);
     float4 imin = d.bmin[iBlock], imax = d.bmax[iBlock];
     const int j0 = code == 0 ? iBlock : d.repBlockStart[r];
     const int j1 = d.repBlockStart[r + 1];

@@ -47,12 +47,6 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
   return y;
 }
 
-__device__ __forceinline__ void shift_of(int code, int &sx, int &sy, int &sz) {
-  if (code < 2) { sx = code; sy = 0; sz = 0; }
-  else if (code < 5) { sx = code - 3; sy = 1; sz = 0; }
-  else { int c = code - 5; sx = c % 3 - 1; sy = c / 3 - 1; sz = 1; }
-}
-
 __device__ __forceinline__ bool aabb_hit(float4 imin, float4 imax, float4 jmin, float4 jmax,
                                          float3 sh, float c2) {
   float g, acc = 0.f, lo, hi;
@@ -431,19 +425,18 @@ __device__ __forceinline__ void plain_loop(JRegs<COMBINE, ALCH> &J, const float4
 // item is padded.
 // ---------------------------------------------------------------------------
 template <bool COMBINE>
-__device__ __forceinline__ void stream_load(const Dev &d, int e, float bx, float by, float bz, float &x, float &y,
+__device__ __forceinline__ void stream_load(const Dev &d, int e, const float4 *shifts, float &x, float &y,
                                             float &z, float &q, int &t, float &ex, float &er) {
   if (e < 0) {  // padding: far outside rCut of every i atom
     x = 1.0e18f; y = 0.f; z = 0.f; q = 0.f; t = 0; ex = 0.f; er = 0.f;
     return;
   }
   const int js = e & 0x7FFFFFF;
-  int sx, sy, sz;
-  shift_of(e >> 27, sx, sy, sz);
+  const float4 sh = shifts[e >> 27];
   const float4 xj = d.xyzq[js];
-  x = xj.x + (float)sx * bx;
-  y = xj.y + (float)sy * by;
-  z = xj.z + (float)sz * bz;
+  x = xj.x + sh.x;
+  y = xj.y + sh.y;
+  z = xj.z + sh.z;
   q = xj.w;
   t = d.slotType[js];
   if (COMBINE) {
@@ -455,8 +448,8 @@ __device__ __forceinline__ void stream_load(const Dev &d, int e, float bx, float
 
 template <int ELEC, int VDW, bool ENERGY, bool COMBINE>
 __device__ __forceinline__ void stream_chunk(const Dev &d, const PairConst &pc, const float2 *sLJ, const int *sS,
-                                             int C, int lane, float4 xi, int rowI, float2 ljI, float bx, float by,
-                                             float bz, float2 &fix2, float2 &fiy2, float2 &fiz2, long long &ei,
+                                             int C, int lane, float4 xi, int rowI, float2 ljI, const float4 *shifts,
+                                             float2 &fix2, float2 &fiy2, float2 &fiz2, long long &ei,
                                              unsigned long long &pairs, int count) {
   const int gj = C > 32 ? 32 : (C > 16 ? 16 : (C > 8 ? 8 : 4));
   const int cl = lane & (gj - 1);
@@ -464,8 +457,8 @@ __device__ __forceinline__ void stream_chunk(const Dev &d, const PairConst &pc, 
   const int eB = gj + cl < C ? sS[gj + cl] : -1;
   float2 jx, jy, jz, jq, jex = f2(0.f), jer = f2(0.f);
   int tA, tB;
-  stream_load<COMBINE>(d, eA, bx, by, bz, jx.x, jy.x, jz.x, jq.x, tA, jex.x, jer.x);
-  stream_load<COMBINE>(d, eB, bx, by, bz, jx.y, jy.y, jz.y, jq.y, tB, jex.y, jer.y);
+  stream_load<COMBINE>(d, eA, shifts, jx.x, jy.x, jz.x, jq.x, tA, jex.x, jer.x);
+  stream_load<COMBINE>(d, eB, shifts, jx.y, jy.y, jz.y, jq.y, tB, jex.y, jer.y);
   float2 jfx = f2(0.f), jfy = f2(0.f), jfz = f2(0.f);
   const float2 xi2 = f2(xi.x), yi2 = f2(xi.y), zi2 = f2(xi.z), qi2 = f2(xi.w);
   const float2 m1 = f2(-1.f);
@@ -607,7 +600,7 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
     const int bi = ALCH ? d.slotSiteBlock[islot] : 0;
     const float li = (ALCH && bi) ? sLam[bi & 0xFFFF] : 1.f;
     const RepInfo &ri = d.rep[d.blockRep[iBlock]];
-    const float bx = ri.box[0], by = ri.box[1], bz = ri.box[2];
+    const float4 *shifts = ri.shift;  // image shift vectors by shift code
     const float4 imin = d.bmin[iBlock], imax = d.bmax[iBlock];
 
     // per-step recull of this work item's candidates (recull.cu:41-122)
@@ -615,10 +608,8 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
     bool hit = false;
     if (c0 + lane < c1) {
       cand = d.cand[c0 + lane];
-      int sx, sy, sz;
-      shift_of(cand.y, sx, sy, sz);
-      float3 sh = make_float3(__fmul_rn((float)sx, bx), __fmul_rn((float)sy, by),
-                              __fmul_rn((float)sz, bz));
+      const float4 sv = shifts[cand.y];
+      const float3 sh = make_float3(sv.x, sv.y, sv.z);
       hit = aabb_hit(imin, imax, d.bmin[cand.x], d.bmax[cand.x], sh, pc.rc2);
     }
     unsigned act = __ballot_sync(kFull, hit);
@@ -638,9 +629,8 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
       const int jBlock = cur.jBlock;
       const int code = cur.code;
       const int mIdx = cur.mIdx;
-      int sx, sy, sz;
-      shift_of(code, sx, sy, sz);
-      const float shx = (float)sx * bx, shy = (float)sy * by, shz = (float)sz * bz;
+      const float4 sv = shifts[code];
+      const float shx = sv.x, shy = sv.y, shz = sv.z;
       const int jslot = 32 * jBlock + lane;
       const float jx = cur.xj.x + shx, jy = cur.xj.y + shy, jz = cur.xj.z + shz;
       const int bj0 = ALCH ? cur.siteBlock : 0;
@@ -672,7 +662,7 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
         nS += nj;
         __syncwarp();
         if (nS >= 64) {
-          stream_chunk<ELEC, VDW, ENERGY, COMBINE>(d, pc, sLJ, sStream[warp], 64, lane, xi, rowI, ljI, bx, by, bz,
+          stream_chunk<ELEC, VDW, ENERGY, COMBINE>(d, pc, sLJ, sStream[warp], 64, lane, xi, rowI, ljI, shifts,
                                                    fix2, fiy2, fiz2, ei, pairs, A.count);
           const int rest = nS - 64;  // < 32
           const int carry = lane < rest ? sStream[warp][64 + lane] : 0;
@@ -816,8 +806,8 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
       const int rem = nS - off;
       const int cap = rem > 48 ? 64 : (rem > 24 ? 32 : (rem > 12 ? 16 : 8));
       const int cnt = rem < cap ? rem : cap;
-      stream_chunk<ELEC, VDW, ENERGY, COMBINE>(d, pc, sLJ, sStream[warp] + off, cnt, lane, xi, rowI, ljI, bx, by,
-                                               bz, fix2, fiy2, fiz2, ei, pairs, A.count);
+      stream_chunk<ELEC, VDW, ENERGY, COMBINE>(d, pc, sLJ, sStream[warp] + off, cnt, lane, xi, rowI, ljI, shifts,
+                                               fix2, fiy2, fiz2, ei, pairs, A.count);
       off += cnt;
     }
     __syncwarp();  // sStream is rewritten by the next work item

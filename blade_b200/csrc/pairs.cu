@@ -86,9 +86,20 @@ __device__ __forceinline__ float3 min_image(const PairsArgs &a, int ii, int jj, 
   const RepInfo &ri = a.rep[a.atomRep[ii]];
   float3 d = make_float3(a.x[3 * ii] - a.x[3 * jj], a.x[3 * ii + 1] - a.x[3 * jj + 1],
                          a.x[3 * ii + 2] - a.x[3 * jj + 2]);
-  d.x -= ri.box[0] * rintf(d.x / ri.box[0]);
-  d.y -= ri.box[1] * rintf(d.y / ri.box[1]);
-  d.z -= ri.box[2] * rintf(d.z / ri.box[2]);
+  if (ri.tric[0] == 0.f && ri.tric[1] == 0.f && ri.tric[2] == 0.f) {
+    d.x -= ri.box[0] * rintf(d.x / ri.box[0]);
+    d.y -= ri.box[1] * rintf(d.y / ri.box[1]);
+    d.z -= ri.box[2] * rintf(d.z / ri.box[2]);
+  } else {  // triclinic: by C, then B, then A (real3_subpbc<true>, src/main/real3.h:215-240)
+    float i = rintf(d.z / ri.box[2]);
+    d.x -= ri.tric[1] * i;
+    d.y -= ri.tric[2] * i;
+    d.z -= ri.box[2] * i;
+    i = rintf(d.y / ri.box[1]);
+    d.x -= ri.tric[0] * i;
+    d.y -= ri.box[1] * i;
+    d.x -= ri.box[0] * rintf(d.x / ri.box[0]);
+  }
   r = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
   return d;
 }

@@ -71,7 +71,14 @@ class NbDirect:
         _lib.call("bnb_create", C.byref(self.params), self.R, self.counts.ctypes.data_as(C.c_void_p), C.byref(h))
         self.h = h
         self._set_topology()
-        self.boxes = np.concatenate([np.asarray(s.box, np.float32) for s in self.systems]).astype(np.float32)
+        # triclinic cells (any replica): every boxes argument is State::tricBox_f
+        # per replica (A_x, B_x, B_y, C_x, C_y, C_z); bnb_set_box_type
+        self.triclinic = any(s.tric is not None for s in self.systems)
+        if self.triclinic:
+            _lib.call("bnb_set_box_type", self.h, 1)
+            self.boxes = np.concatenate([s.tric_box() for s in self.systems]).astype(np.float32)
+        else:
+            self.boxes = np.concatenate([np.asarray(s.box, np.float32) for s in self.systems]).astype(np.float32)
 
     # -- topology --------------------------------------------------------------
     def _set_topology(self):

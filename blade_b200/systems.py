@@ -11,6 +11,7 @@ parameter distributions of the workloads:
 * ``msld_water``    the water box plus MSLD perturbation sites
   (3 sites x 4 substituents of 8-15 atoms).
 * ``batch_replicas`` uneven chain-in-water MSLD replicas, 3k-30k atoms.
+* ``water_box_tric`` TIP3P waters in a triclinic cell (State::tricBox layout).
 * ``load_fixture``  the reference's own water216 and newDHFR fixtures, as the
   golden-vector script stored them (tests/golden/fixture_*.npz).
 
@@ -76,6 +77,18 @@ class System:
     bonds: np.ndarray | None = None      # [B,2] int32 covalent bonds (one order), for dynamics only
     bond_param: np.ndarray | None = None  # [B,2] float32 (kb, b0): U = kb/2 (r - b0)^2
     masses: np.ndarray | None = None      # [N] amu, when the system comes with its own
+    tric: np.ndarray | None = None        # [3] (B_x, C_x, C_y) of a triclinic cell, else None
+
+    def box6(self) -> np.ndarray:
+        """(A_x, B_y, C_z, B_x, C_x, C_y): box edges, then the off-diagonal
+        components of the lower-triangular cell (zero when orthorhombic)."""
+        t = np.zeros(3, np.float32) if self.tric is None else np.asarray(self.tric, np.float32)
+        return np.concatenate([np.asarray(self.box, np.float32), t]).astype(np.float32)
+
+    def tric_box(self) -> np.ndarray:
+        """The cell in the layout of State::tricBox_f: A_x, B_x, B_y, C_x, C_y, C_z."""
+        b = self.box6()
+        return np.array([b[0], b[3], b[1], b[4], b[5], b[2]], np.float32)
 
     @property
     def N(self) -> int:
@@ -301,6 +314,30 @@ def water_box(seed: int = 1, n_side: int = 6, box: float = 18.856, jitter: float
     vdw = vdw_table([TIP3P_EPS_H, TIP3P_EPS_O], [TIP3P_RH_H, TIP3P_RH_O])
     return System("water216", xyz, np.float32([box] * 3), nb, vdw, water_excl(0, nw),
                   rCut, rSwitch, beta)
+
+
+def water_box_tric(seed: int = 6, cell=(24.0, 7.0, 23.0, -6.0, 8.0, 22.5), n=(8, 8, 7), jitter: float = 0.3,
+                   rCut: float = 9.0, rSwitch: float = 8.0, beta: float = 0.34) -> System:
+    """TIP3P waters on a lattice spanning a triclinic cell, given in the layout
+    of State::tricBox_f (A_x, B_x, B_y, C_x, C_y, C_z): A = (A_x,0,0),
+    B = (B_x,B_y,0), C = (C_x,C_y,C_z).  Sites at fractional coordinates
+    ((i+1/2)/n0, (j+1/2)/n1, (k+1/2)/n2), seeded orientations and jitter;
+    coordinates are left unwrapped (inside the parallelepiped, not the brick)."""
+    rng = np.random.default_rng(seed)
+    ax, bx, by, cx, cy, cz = (float(v) for v in cell)
+    A, B, C = np.array([ax, 0, 0]), np.array([bx, by, 0]), np.array([cx, cy, cz])
+    f = [(np.arange(k) + 0.5) / k for k in n]
+    u = np.stack(np.meshgrid(*f, indexing="ij"), -1).reshape(-1, 3)
+    sites = u[:, :1] * A + u[:, 1:2] * B + u[:, 2:3] * C
+    xyz = place_waters(rng, sites, jitter).astype(np.float32)
+    nw = len(sites)
+    nb = np.zeros(3 * nw, NBOND_DTYPE)
+    nb["q"] = np.tile(np.float32([TIP3P_Q_O, TIP3P_Q_H, TIP3P_Q_H]), nw)
+    nb["typeIdx"] = np.tile(np.int32([1, 0, 0]), nw)
+    vdw = vdw_table([TIP3P_EPS_H, TIP3P_EPS_O], [TIP3P_RH_H, TIP3P_RH_O])
+    s = System("water_tric", xyz, np.float32([ax, by, cz]), nb, vdw, water_excl(0, nw), rCut, rSwitch, beta)
+    s.tric = np.float32([bx, cx, cy])
+    return s
 
 
 def _fill_water(rng, box: float, nwat: int, solute: np.ndarray, dmin: float = 2.6):

@@ -100,11 +100,28 @@ int bnb_set_topology(bnb_handle *h, const bnb_nbond *nbonds,
                      const int *exclReplica);
 
 /*
+ * Box shape of every boxes argument of this handle (State::typeBox,
+ * src/system/state.h): 0 (default) orthorhombic, boxes are host float
+ * [3*replicas] edge lengths (State::orthBox_f); 1 triclinic, boxes are host
+ * float [6*replicas] in the layout of State::tricBox_f: A_x, B_x, B_y, C_x,
+ * C_y, C_z of the lower-triangular cell A = (A_x,0,0), B = (B_x,B_y,0),
+ * C = (C_x,C_y,C_z).  Atoms are wrapped into the brick A_x x B_y x C_z as the
+ * reference's triclinic modulus does (src/main/real3.h:340-360), and the
+ * half-shell images are centred under the shear as its cull does
+ * (src/domdec/cull.cu:141-190); A_x, B_y and C_z must each be at least
+ * 2 rCut.  Direct space, nb14/nbex and the list are supported; PME is not
+ * (BNB_ERR_UNSUPPORTED from bnb_set_pme / bnb_compute_pme, and from this call
+ * once PME is set).  Changing the type requires a synchronous rebuild.
+ */
+int bnb_set_box_type(bnb_handle *h, int triclinic);
+
+/*
  * Rebuilds the block list from coordinates (the counterpart of
  * Domdec::reset_domdec, src/domdec/domdec.cu:201-211: bin, sort, 32-atom
  * blocks, AABBs, half-shell cull at rCut+cullPad, exclusion masks).
  * position: device float [3N] (State::position_fd layout, all replicas).
- * boxes: host float [3*replicas] orthorhombic edges.
+ * boxes: host float [3*replicas] orthorhombic edges, or [6*replicas]
+ * triclinic cells after bnb_set_box_type(h, 1).
  * flags: 0 = synchronise and grow capacities on overflow (as the reference's
  * cull loop, src/domdec/cull.cu:337-375); BNB_ASYNC = enqueue only (graph
  * capturable), overflow is reported through bnb_status and the pair kernel

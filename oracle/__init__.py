@@ -51,6 +51,8 @@ def lib():
         _LIB.orc_nbdirect64.argtypes = _LIB.orc_nbdirect.argtypes
         _LIB.orc_nbdirect_window64.argtypes = _LIB.orc_nbdirect.argtypes + [i, i]
         _LIB.orc_nbdirect_brute64.argtypes = _LIB.orc_nbdirect_brute.argtypes
+        _LIB.orc_nbdirect_tric64.argtypes = _LIB.orc_nbdirect_brute.argtypes
+        _LIB.orc_shift_table.argtypes = [p, p]
         _LIB.orc_pair.argtypes = [d, d, d, d, d, i, i, d, d, C.POINTER(_Params), p, p, p, p]
         _LIB.orc_lambda_from_theta.argtypes = [i, p, d, p, p, p]
         _LIB.orc_thetaForce_from_lambdaForce.argtypes = [i, p, p, d, p, p, p, p, p]
@@ -95,7 +97,13 @@ def nbdirect(sys, lam=None, xyz=None, brute=False, nthreads=0, calc_alch=None):
     e = np.zeros(1)
     cnt = np.zeros(1, np.int64)
     p = params(sys, calc_alch)
-    if brute:
+    if sys.tric is not None:           # triclinic cell: all-pairs over lattice images
+        x64 = np.ascontiguousarray(xyz, np.float64)
+        b6 = np.ascontiguousarray(sys.box6(), np.float64)
+        rc = lib().orc_nbdirect_tric64(N, _ptr(x64), _ptr(b6), _ptr(nb), sys.nTypes, _ptr(vdw), len(excl),
+                                       _ptr(excl), C.byref(p), _ptr(lam), len(lam), _ptr(g), _ptr(lf), _ptr(e),
+                                       _ptr(cnt))
+    elif brute:
         fn = lib().orc_nbdirect_brute64 if f64 else lib().orc_nbdirect_brute
         rc = fn(N, _ptr(xyz), _ptr(box), _ptr(nb), sys.nTypes, _ptr(vdw), len(excl), _ptr(excl),
                 C.byref(p), _ptr(lam), len(lam), _ptr(g), _ptr(lf), _ptr(e), _ptr(cnt))
@@ -194,7 +202,7 @@ def build_list(sys, xyz=None, rcull=None):
     """FP32/integer block list: same structures as the CUDA builder exports."""
     from blade_b200.systems import excl_csr
     xyz = np.ascontiguousarray(sys.xyz if xyz is None else xyz, np.float32)
-    box = np.ascontiguousarray(sys.box, np.float32)
+    box = np.ascontiguousarray(sys.box6(), np.float32)
     N = xyz.shape[0]
     es, ea = excl_csr(N, sys.excl)
     rc = np.float32(sys.rCut) + np.float32(sys.cullPad) if rcull is None else np.float32(rcull)
@@ -225,8 +233,23 @@ def shift_vector(code):
     return int(x[0]), int(y[0]), int(z[0])
 
 
+def box6_of(box):
+    """A box argument as the 6-float cell (A_x, B_y, C_z, B_x, C_x, C_y):
+    3 edges (orthorhombic) are padded with zeros."""
+    b = np.asarray(box, np.float32).reshape(-1)
+    return np.ascontiguousarray(np.concatenate([b, np.zeros(6 - len(b), np.float32)]) if len(b) < 6 else b[:6])
+
+
+def shift_table(box):
+    """[14,3] image shift vectors of the half-shell codes for a box (3 or 6 floats)."""
+    t = np.zeros((14, 3), np.float32)
+    lib().orc_shift_table(_ptr(box6_of(box)), _ptr(t))
+    return t
+
+
 def pack(lst, xyz, box):
-    """Pack with stored wrap shifts; returns packed [32B,3] and AABBs."""
+    """Pack with stored wrap shifts; returns packed [32B,3] and AABBs.
+    box: 3 edges or the 6-float cell."""
     B = lst["blockCount"]
     L = _List()
     L.N = len(xyz)
@@ -236,7 +259,7 @@ def pack(lst, xyz, box):
     L.wrap = wrap.ctypes.data_as(C.POINTER(C.c_int))
     L.slotAtom = slot.ctypes.data_as(C.POINTER(C.c_int))
     x = np.ascontiguousarray(xyz, np.float32)
-    b = np.ascontiguousarray(box, np.float32)
+    b = box6_of(box)
     packed = np.zeros((32 * B, 3), np.float32)
     mn = np.zeros((B, 3), np.float32)
     mx = np.zeros((B, 3), np.float32)
@@ -248,11 +271,11 @@ def active_tiles(lst, bmin, bmax, box, rcut):
     """Per-step recull at rCut: boolean per candidate (recull.cu:41-122)."""
     c2 = np.float32(np.float32(rcut) * np.float32(rcut))
     out = np.zeros(len(lst["cand"]), bool)
-    box = np.asarray(box, np.float32)
+    table = shift_table(box)
     for i in range(lst["blockCount"]):
         for c in range(lst["candStart"][i], lst["candStart"][i + 1]):
             j, code = lst["cand"][c]
-            s = np.float32(shift_vector(int(code))) * box
+            s = table[int(code)]
             out[c] = bool(lib().orc_aabb_hit(_ptr(np.ascontiguousarray(bmin[i])),
                                              _ptr(np.ascontiguousarray(bmax[i])),
                                              _ptr(np.ascontiguousarray(bmin[j])),
@@ -270,7 +293,7 @@ def pair_lists(sys, xyz=None, lam=None, which="nb14", soft14=False):
     """FP64 nb14 or nbex energy, gradient dU/dx [N,3] and dU/dlambda
     (src/bonded/pair.cu) for the system's pair lists."""
     xyz = np.ascontiguousarray(sys.xyz if xyz is None else xyz, np.float64)
-    box = np.ascontiguousarray(sys.box, np.float64)
+    box = np.ascontiguousarray(sys.box6(), np.float64)
     lam = np.ascontiguousarray(sys.lambdas() if lam is None else lam, np.float64)
     g = np.zeros((xyz.shape[0], 3))
     lf = np.zeros(len(lam))

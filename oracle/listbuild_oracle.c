@@ -70,13 +70,53 @@ static inline uint32_t zkey(float z) {
   return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
-static inline float wrap_coord(float x, float L, int *s) {
-  float q = x / L;
-  float f = floorf(q);
-  f = f < -127.0f ? -127.0f : (f > 127.0f ? 127.0f : f);
-  *s = (int)f;
-  float sl = f * L;
-  return x - sl;
+/* Box of 6 floats: A_x, B_y, C_z (the brick) then B_x, C_x, C_y (zero for an
+ * orthorhombic box): A = (A_x,0,0), B = (B_x,B_y,0), C = (C_x,C_y,C_z). */
+static inline float clamp_shift(float f) { return f < -127.0f ? -127.0f : (f > 127.0f ? 127.0f : f); }
+
+/* Lattice translation sx A + sy B + sz C, one rounding per operation in the
+ * order of the reference's shift (src/nbdirect/nbdirect.cu:196-199). */
+void orc_lattice_shift(const float box[6], int sx, int sy, int sz, float out[3]) {
+  float fx = (float)sx, fy = (float)sy, fz = (float)sz;
+  float t0 = fz * box[4], t1 = fy * box[3], t2 = fx * box[0];
+  float s0 = t0 + t1;
+  out[0] = s0 + t2;
+  float u0 = fz * box[5], u1 = fy * box[1];
+  out[1] = u0 + u1;
+  out[2] = fz * box[2];
+}
+
+/* Integer image shift of a position: z by C, then y by B, then x by A (the
+ * reference's triclinic modulus, src/main/real3.h:340-360). */
+static inline void wrap_shift(const float *x, const float box[6], int s[3]) {
+  float fz = clamp_shift(floorf(x[2] / box[2]));
+  float t = fz * box[5];
+  float yz = x[1] - t;
+  t = fz * box[4];
+  float xz = x[0] - t;
+  float fy = clamp_shift(floorf(yz / box[1]));
+  t = fy * box[3];
+  float xy = xz - t;
+  float fx = clamp_shift(floorf(xy / box[0]));
+  s[0] = (int)fx; s[1] = (int)fy; s[2] = (int)fz;
+}
+
+/* Shift vectors of the 14 half-shell codes, centred under the shear as the
+ * reference's cull (src/domdec/cull.cu:141-190). */
+void orc_shift_table(const float box[6], float table[14][3]) {
+  for (int code = 0; code < 14; code++) {
+    int x, y, z;
+    orc_shift_vector(code, &x, &y, &z);
+    float ty = (float)z * box[5];
+    float qy = ty / box[1];
+    int y0 = -(int)floorf(qy + 0.5f);
+    int sy = y + y0;
+    float tx0 = (float)z * box[4], tx1 = (float)sy * box[3];
+    float sxy = tx0 + tx1;
+    float qx = sxy / box[0];
+    int x0 = -(int)floorf(qx + 0.5f);
+    orc_lattice_shift(box, x + x0, sy, z, table[code]);
+  }
 }
 
 typedef struct { uint64_t key; int col; int atom; } sort_rec;
@@ -87,12 +127,7 @@ static int cmp_rec(const void *a, const void *b) {
   return 0;
 }
 
-static inline float unwrap_pack(float x, int s, float L) {
-  float sl = (float)s * L;
-  return x - sl;
-}
-
-void orc_pack(const orc_list *l, const float *xyz, const float box[3],
+void orc_pack(const orc_list *l, const float *xyz, const float box[6],
               float *packed, float *bmin, float *bmax) {
   int B = l->blockCount;
   for (int b = 0; b < B; b++) {
@@ -105,9 +140,10 @@ void orc_pack(const orc_list *l, const float *xyz, const float box[3],
         continue;
       }
       int w = l->wrap[a];
-      int s[3] = {(w & 0xFF) - 128, ((w >> 8) & 0xFF) - 128, ((w >> 16) & 0xFF) - 128};
+      float L[3];
+      orc_lattice_shift(box, (w & 0xFF) - 128, ((w >> 8) & 0xFF) - 128, ((w >> 16) & 0xFF) - 128, L);
       for (int d = 0; d < 3; d++) {
-        float v = unwrap_pack(xyz[3 * a + d], s[d], box[d]);
+        float v = xyz[3 * a + d] - L[d];
         packed[3 * slot + d] = v;
         if (v < mn[d]) mn[d] = v;
         if (v > mx[d]) mx[d] = v;
@@ -117,7 +153,7 @@ void orc_pack(const orc_list *l, const float *xyz, const float box[3],
   }
 }
 
-int orc_build_list(int N, const float *xyz, const float box[3], float rCull,
+int orc_build_list(int N, const float *xyz, const float box[6], float rCull,
                    const int *exclStart, const int *exclAtom, orc_list *out) {
   memset(out, 0, sizeof(*out));
   out->N = N;
@@ -129,8 +165,10 @@ int orc_build_list(int N, const float *xyz, const float box[3], float rCull,
   out->colCount = (int *)calloc(nCols, sizeof(int));
   for (int a = 0; a < N; a++) {
     int s[3];
-    float w[3];
-    for (int d = 0; d < 3; d++) w[d] = wrap_coord(xyz[3 * a + d], box[d], &s[d]);
+    float w[3], L[3];
+    wrap_shift(&xyz[3 * a], box, s);
+    orc_lattice_shift(box, s[0], s[1], s[2], L);
+    for (int d = 0; d < 3; d++) w[d] = xyz[3 * a + d] - L[d];
     out->wrap[a] = (s[0] + 128) | ((s[1] + 128) << 8) | ((s[2] + 128) << 16);
     float px = w[0] / box[0];
     int ix = (int)floorf(px * (float)divX);
@@ -188,12 +226,12 @@ int orc_build_list(int N, const float *xyz, const float box[3], float rCull,
   int *candExcl = (int *)malloc(sizeof(int) * cap);
   uint32_t *masks = (uint32_t *)malloc(sizeof(uint32_t) * 32 * mcap);
   out->candStart = (int *)malloc(sizeof(int) * (B + 1));
+  float table[14][3];
+  orc_shift_table(box, table);
   for (int i = 0; i < B; i++) {
     out->candStart[i] = cnt;
     for (int code = 0; code < 14; code++) {
-      int sx, sy, sz;
-      orc_shift_vector(code, &sx, &sy, &sz);
-      float sh[3] = {(float)sx * box[0], (float)sy * box[1], (float)sz * box[2]};
+      const float *sh = table[code];
       for (int j = (code == 0 ? i : 0); j < B; j++) {
         if (!orc_aabb_hit(&out->bmin[3 * i], &out->bmax[3 * i], &out->bmin[3 * j],
                           &out->bmax[3 * j], sh, c2))

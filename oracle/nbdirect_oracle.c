@@ -351,6 +351,67 @@ int orc_nbdirect(int N, const float *xyz, const double box[3],
   return rc;
 }
 
+/* Triclinic cell (box6: A_x, B_y, C_z, B_x, C_x, C_y): every pair i<j over
+ * all lattice images within rCut.  The difference is first reduced as the
+ * reference's real3_subpbc<true> (src/main/real3.h:215-240: by C, then B,
+ * then A), then the 27 images around it are tested; with A_x, B_y, C_z >=
+ * 2 rCut at most one of them lies inside rCut. */
+int orc_nbdirect_tric64(int N, const double *xyz, const double box6[6],
+                        const orc_nbond *nb, int nTypes, const orc_vdw *vdw,
+                        int exclCount, const int *excl, const orc_params *p,
+                        const double *lambda, int nLambda,
+                        double *grad, double *lambdaForce, double *energy,
+                        long long *pairCount) {
+  const double ax = box6[0], by = box6[1], cz = box6[2], bx = box6[3], cx = box6[4], cy = box6[5];
+  if (ax < 2 * p->rCut || by < 2 * p->rCut || cz < 2 * p->rCut) return -1;
+  excl_set ex = make_excl(exclCount, excl);
+  memset(grad, 0, sizeof(double) * 3 * N);
+  if (lambdaForce && nLambda > 0) memset(lambdaForce, 0, sizeof(double) * nLambda);
+  const double rc2 = p->rCut * p->rCut;
+  double e = 0;
+  long long n = 0;
+  for (int i = 0; i < N; i++)
+    for (int j = i + 1; j < N; j++) {
+      double d0[3] = {xyz[3 * i] - xyz[3 * j], xyz[3 * i + 1] - xyz[3 * j + 1], xyz[3 * i + 2] - xyz[3 * j + 2]};
+      double k = floor(d0[2] / cz + 0.5);
+      d0[0] -= cx * k; d0[1] -= cy * k; d0[2] -= cz * k;
+      k = floor(d0[1] / by + 0.5);
+      d0[0] -= bx * k; d0[1] -= by * k;
+      d0[0] -= ax * floor(d0[0] / ax + 0.5);
+      for (int c = -1; c <= 1; c++)
+        for (int b = -1; b <= 1; b++)
+          for (int a = -1; a <= 1; a++) {
+            const double dx = d0[0] + a * ax + b * bx + c * cx;
+            const double dy = d0[1] + b * by + c * cy;
+            const double dz = d0[2] + c * cz;
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            if (!(r2 < rc2) || is_excluded(&ex, i, j)) continue;
+            const double r = sqrt(r2);
+            const orc_nbond A = nb[i], Bn = nb[j];
+            const orc_vdw v = vdw[A.typeIdx * nTypes + Bn.typeIdx];
+            double li = 1, lj = 1;
+            if (p->calcAlch) {
+              if (A.siteBlock) li = lambda[A.siteBlock & 0xFFFF];
+              if (Bn.siteBlock) lj = lambda[Bn.siteBlock & 0xFFFF];
+            }
+            double E, fr, fli, flj;
+            orc_pair(r, A.q, Bn.q, v.c12, v.c6, A.siteBlock, Bn.siteBlock, li, lj, p, &E, &fr, &fli, &flj);
+            grad[3 * i] += fr * dx; grad[3 * i + 1] += fr * dy; grad[3 * i + 2] += fr * dz;
+            grad[3 * j] -= fr * dx; grad[3 * j + 1] -= fr * dy; grad[3 * j + 2] -= fr * dz;
+            if (p->calcAlch) {
+              if (A.siteBlock) lambdaForce[A.siteBlock & 0xFFFF] += fli;
+              if (Bn.siteBlock) lambdaForce[Bn.siteBlock & 0xFFFF] += flj;
+            }
+            e += E;
+            n++;
+          }
+    }
+  *energy = e;
+  if (pairCount) *pairCount = n;
+  free(ex.k);
+  return 0;
+}
+
 int orc_nbdirect_brute(int N, const float *xyz, const double box[3],
                        const orc_nbond *nb, int nTypes, const orc_vdw *vdw,
                        int exclCount, const int *excl, const orc_params *p,
@@ -508,12 +569,15 @@ static void nb14_terms(const orc_nb14 *pp, const orc_params *p, double r, double
   }
 }
 
-static void pl_min_image(const double *xi, const double *xj, const double box[3], double d[3]) {
-  for (int k = 0; k < 3; k++) {
-    double v = xi[k] - xj[k];
-    v -= box[k] * nearbyint(v / box[k]);
-    d[k] = v;
-  }
+/* box: A_x, B_y, C_z, B_x, C_x, C_y; the reference's real3_subpbc (by C, then
+ * B, then A; per axis for an orthorhombic box, src/main/real3.h:215-240). */
+static void pl_min_image(const double *xi, const double *xj, const double box[6], double d[3]) {
+  for (int k = 0; k < 3; k++) d[k] = xi[k] - xj[k];
+  double k = nearbyint(d[2] / box[2]);
+  d[0] -= box[4] * k; d[1] -= box[5] * k; d[2] -= box[2] * k;
+  k = nearbyint(d[1] / box[1]);
+  d[0] -= box[3] * k; d[1] -= box[1] * k;
+  d[0] -= box[0] * nearbyint(d[0] / box[0]);
 }
 
 /* getforce_pair_kernel's scaling, soft core and routing (pair.cu:205-283). */
@@ -541,7 +605,7 @@ static void pair_apply(int ii, int jj, const int sb[2], const double d[3], doubl
   energy[0] += E * l0 * l1;
 }
 
-void orc_nb14_pairs(int n, const orc_nb14 *pp, const double *xyz, const double box[3], const double *lambda,
+void orc_nb14_pairs(int n, const orc_nb14 *pp, const double *xyz, const double box[6], const double *lambda,
                     const orc_params *p, int useSoftCore14, double *grad, double *lambdaForce, double *energy) {
   for (int t = 0; t < n; t++) {
     const int ii = pp[t].idx[0], jj = pp[t].idx[1];
@@ -572,7 +636,7 @@ void orc_nb14_pairs(int n, const orc_nb14 *pp, const double *xyz, const double b
   }
 }
 
-void orc_nbex_pairs(int n, const orc_nbex *pp, const double *xyz, const double box[3], const double *lambda,
+void orc_nbex_pairs(int n, const orc_nbex *pp, const double *xyz, const double box[6], const double *lambda,
                     const orc_params *p, double *grad, double *lambdaForce, double *energy) {
   for (int t = 0; t < n; t++) {
     const int ii = pp[t].idx[0], jj = pp[t].idx[1];

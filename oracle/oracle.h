@@ -73,6 +73,12 @@ int orc_nbdirect64(int N, const double *xyz, const double box[3],
                    const double *lambda, int nLambda,
                    double *grad, double *lambdaForce, double *energy,
                    long long *pairCount, int nthreads);
+int orc_nbdirect_tric64(int N, const double *xyz, const double box6[6],
+                        const orc_nbond *nb, int nTypes, const orc_vdw *vdw,
+                        int exclCount, const int *excl, const orc_params *p,
+                        const double *lambda, int nLambda,
+                        double *grad, double *lambdaForce, double *energy,
+                        long long *pairCount);
 int orc_nbdirect_brute64(int N, const double *xyz, const double box[3],
                          const orc_nbond *nb, int nTypes, const orc_vdw *vdw,
                          int exclCount, const int *excl, const orc_params *p,
@@ -133,12 +139,16 @@ typedef struct {
 void orc_domain_div(int N, const float box[3], int *divX, int *divY);
 /* Build the list with culling distance rCull (=rCut+pad).  The exclusion
  * list is CSR over atoms (exclStart[N+1], exclAtom[]) sorted per atom. */
-int orc_build_list(int N, const float *xyz, const float box[3], float rCull,
+/* box: A_x, B_y, C_z, B_x, C_x, C_y (the last three zero for an orthorhombic
+ * box): the lower-triangular cell of the reference's State::tricBox. */
+int orc_build_list(int N, const float *xyz, const float box[6], float rCull,
                    const int *exclStart, const int *exclAtom, orc_list *out);
 void orc_free_list(orc_list *l);
 /* Pack positions with the stored wrap shift and recompute AABBs
  * (assign_blocks.cu:340-382). */
-void orc_pack(const orc_list *l, const float *xyz, const float box[3],
+void orc_shift_table(const float box[6], float table[14][3]);
+void orc_lattice_shift(const float box[6], int sx, int sy, int sz, float out[3]);
+void orc_pack(const orc_list *l, const float *xyz, const float box[6],
               float *packed /* [32B*3] */, float *bmin, float *bmax);
 /* Shift code (0..13) -> integer shift, half shell of cull.cu:127-173. */
 void orc_shift_vector(int code, int *sx, int *sy, int *sz);
@@ -156,13 +166,14 @@ typedef struct { int idx[2]; int siteBlock[2]; float qxq; } orc_nbex;
  * Nb14Potential (pair.cu:63-187: switched LJ and e14fac-scaled elec) and for
  * NbExPotential (pair.cu:190-202: the PME erf correction of excluded pairs),
  * MSLD scaling l0*l1 and, for nb14 with useSoftCore14, the soft core
- * (pair.cu:205-283).  Minimum image in the orthorhombic box.  Outputs are
+ * (pair.cu:205-283).  Minimum image in the cell box (A_x, B_y, C_z, B_x, C_x,
+ * C_y; the last three zero for an orthorhombic box).  Outputs are
  * ADDED: grad[3N] (dU/dx), lambdaForce, energy[1].
  */
-void orc_nb14_pairs(int n, const orc_nb14 *pp, const double *xyz, const double box[3],
+void orc_nb14_pairs(int n, const orc_nb14 *pp, const double *xyz, const double box[6],
                     const double *lambda, const orc_params *p, int useSoftCore14,
                     double *grad, double *lambdaForce, double *energy);
-void orc_nbex_pairs(int n, const orc_nbex *pp, const double *xyz, const double box[3],
+void orc_nbex_pairs(int n, const orc_nbex *pp, const double *xyz, const double box[6],
                     const double *lambda, const orc_params *p,
                     double *grad, double *lambdaForce, double *energy);
 

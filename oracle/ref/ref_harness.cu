@@ -686,3 +686,20 @@ extern "C" int ref_update_step(ref_handle *h, double *pos, float *vel, float *fr
   cudaFree(pot->branch3Cons_d);
   return rc ? rc : (cudaGetLastError() == cudaSuccess ? 0 : 2);
 }
+
+// Triclinic cell for the handle (State::typeBox = true): tric host double [6]
+// in the layout of State::tricBox (A_x, B_x, B_y, C_x, C_y, C_z), also the
+// FP32 copy tricBox_f the direct-space path reads.
+extern "C" int ref_set_tric(ref_handle *h, const double *tric) {
+  State *st = h->st;
+  st->typeBox = true;
+  st->tricBox.a.x = tric[0];
+  st->tricBox.b.x = tric[1]; st->tricBox.b.y = tric[2];
+  st->tricBox.c.x = tric[3]; st->tricBox.c.y = tric[4]; st->tricBox.c.z = tric[5];
+  st->tricBox_f.a.x = (float)tric[0];
+  st->tricBox_f.b.x = (float)tric[1]; st->tricBox_f.b.y = (float)tric[2];
+  st->tricBox_f.c.x = (float)tric[3]; st->tricBox_f.c.y = (float)tric[4]; st->tricBox_f.c.z = (float)tric[5];
+  st->orthBox.x = tric[0]; st->orthBox.y = tric[2]; st->orthBox.z = tric[5];
+  st->orthBox_f.x = (float)tric[0]; st->orthBox_f.y = (float)tric[2]; st->orthBox_f.z = (float)tric[5];
+  return 0;
+}

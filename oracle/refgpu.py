@@ -36,6 +36,7 @@ def lib():
         L.ref_time_pme.argtypes = [p, i, i, p]
         L.ref_holonomic.argtypes = [p, i, i, p, i, p, i, p, i, p, p, p, p, p, f, f]
         L.ref_set_msld.argtypes = [p, i, p, p, p, p, i, p, f]
+        L.ref_set_tric.argtypes = [p, p]
         L.ref_msld_lambda.argtypes = [p, p, p]
         L.ref_msld_theta_force.argtypes = [p, p, p, p, p]
         L.ref_msld_bias.argtypes = [p, p, i, p, p]
@@ -67,6 +68,9 @@ class RefGPU:
         if rc != 0:
             raise RuntimeError("reference harness: create failed")
         self.h = h
+        if getattr(sys, "tric", None) is not None:   # State::typeBox = true, tricBox from the cell
+            self._tric = np.ascontiguousarray(sys.tric_box(), np.float64)
+            lib().ref_set_tric(self.h, self._tric.ctypes.data_as(C.c_void_p))
 
     def set_state(self, xyz=None, lam=None):
         P = lambda a: None if a is None else np.ascontiguousarray(a, np.float64).ctypes.data_as(C.c_void_p)

@@ -27,7 +27,9 @@ msld_maps*.npz and update_msld_water.npz (--msld-only makes just these);
 and the reference's own CHARMM fixtures: `make_golden.py REFERENCE_ROOT
 --fixtures` (CPU) turns test/water216 and test/newDHFR into
 fixture_<name>.npz, and `--real-only` (GPU) evaluates the reference's direct
-space, nb14, nbex, PME and self terms on them into real_<name>.npz.
+space, nb14, nbex, PME and self terms on them into real_<name>.npz; and the
+reference's triclinic direct space on triclinic water boxes, tric_*.npz
+(--tric-only).
 """
 import os
 import sys
@@ -225,8 +227,27 @@ def real_cases(out):
         print("real", name, r["energy"], r14["energy"], rex["energy"], rp["energy"], rs["energy"], K, flush=True)
 
 
-def main(out, pairs_only=False, pme_only=False, holonomic_only=False, msld_only=False, real_only=False):
+def tric_cases(out):
+    """The reference's triclinic direct space (State::typeBox, the flagBox
+    branch of getforce_nbdirect and Domdec) on the triclinic water box, plain
+    and with two MSLD sites."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from test_gpu_triclinic import CASES
+    for name, make in CASES.items():
+        s = make()
+        r = refgpu.RefGPU(s).evaluate()
+        np.savez_compressed(os.path.join(out, f"tric_{name}.npz"), case=np.str_(name), xyz=s.xyz.astype(np.float32),
+                            grad=r["grad"].astype(np.float32), energy=np.float64(r["energy"]),
+                            lambdaForce=r["lambdaForce"].astype(np.float64), tric_box=s.tric_box())
+        print("tric", name, s.N, r["energy"], flush=True)
+
+
+def main(out, pairs_only=False, pme_only=False, holonomic_only=False, msld_only=False, real_only=False,
+         tric_only=False):
     os.makedirs(out, exist_ok=True)
+    if tric_only:
+        tric_cases(out)
+        return
     if real_only:
         real_cases(out)
         return
@@ -278,4 +299,5 @@ if __name__ == "__main__":
         sys.exit(0)
     main(args[0] if args else os.path.join(ROOT, "golden_out"), pairs_only="--pairs-only" in sys.argv,
          pme_only="--pme-only" in sys.argv, holonomic_only="--holonomic-only" in sys.argv,
-         msld_only="--msld-only" in sys.argv, real_only="--real-only" in sys.argv)
+         msld_only="--msld-only" in sys.argv, real_only="--real-only" in sys.argv,
+         tric_only="--tric-only" in sys.argv)
