@@ -95,7 +95,9 @@ def trajectory_np(s, k: int, seed: int):
 # clocks
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    """Samples SM clock and clock-event reasons through NVML during a region."""
+    """Samples SM clock and clock-event reasons through NVML during a region
+    (every millisecond; the timed loop also runs the counting pass and the
+    e2e leg inside one sampler, so a short timed region still has samples)."""
 
     REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
                "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80}
@@ -124,7 +126,7 @@ class ClockSampler:
                         self.reasons.add(k)
             except Exception:
                 pass
-            time.sleep(0.005)
+            time.sleep(0.001)
 
     def __enter__(self):
         if self.ok:
@@ -296,14 +298,14 @@ def run_bnb(args, rank, world):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(dev.index)
-    with clocks:
-        for k in range(K):
-            flush.zero_()
-            evs[k][0].record(stream)
-            step(k, frames[W + k])
-            evs[k][1].record(stream)
-        torch.cuda.synchronize()
+    clocks = ClockSampler(dev.index)   # runs through the timed loop and the e2e leg below
+    clocks.__enter__()
+    for k in range(K):
+        flush.zero_()
+        evs[k][0].record(stream)
+        step(k, frames[W + k])
+        evs[k][1].record(stream)
+    torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     ms = [a.elapsed_time(b) for a, b in evs]
@@ -364,6 +366,7 @@ def run_bnb(args, rank, world):
         torch.cuda.synchronize()
         t_e2e = sum(a.elapsed_time(b) for a, b in e_evs) / 1e3
         e2e = {"t": t_e2e, "h2d": 4 * 3 * s.N, "d2h": 4 * 3 * s.N + 8}
+    clocks.__exit__(None, None, None)
 
     # the reference's own CUDA path (src/nbdirect + src/domdec, unmodified,
     # oracle/_ref) on the same trajectory, same GPU, same L2 flushing

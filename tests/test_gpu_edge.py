@@ -1,5 +1,7 @@
 """GPU edge cases: capacity overflow and regrowth, asynchronous overflow
 reporting, non-finite input, tiny and uneven systems, MSLD lambda kernels."""
+import dataclasses
+
 import numpy as np
 import pytest
 import torch
@@ -183,3 +185,38 @@ def test_output_modes(cuda):
     with pytest.raises(_lib.BnbError):
         nb.getforce_nbdirect(pos, lam, True, force64=g, mode=8)
     nb.close()
+
+
+def test_pair_erfc_path_against_fp64(cuda):
+    """One charge pair at distances across [0.7 A, rCut): the device path
+    erfc(beta r) = ex2(-beta^2 r^2 log2 e) P6(rcp(1 + p beta r)) with rsqrt,
+    in the PME real-space energy and force, against FP64 erfc."""
+    from math import erfc, exp, pi, sqrt
+    s = systems.water_box()
+    nb0 = np.zeros(2, systems.NBOND_DTYPE)
+    nb0["q"] = (0.83, -0.61)
+    vdw = np.zeros((1, 1, 2), np.float32)            # no LJ: the Coulomb term alone
+    k, beta, rc = 332.0716, 0.32, 12.0
+    worst_e = worst_f = 0.0
+    for r in np.concatenate([np.linspace(0.7, 11.9, 57), [11.99]]):
+        xyz = np.array([[20.0, 20.0, 20.0], [20.0 + r * 0.6, 20.0 + r * 0.8, 20.0]], np.float32)
+        t = dataclasses.replace(s, xyz=xyz, box=np.float32([40.0, 40.0, 40.0]), nbonds=nb0, vdw=vdw,
+                                excl=np.zeros((0, 2), np.int32), rCut=rc, rSwitch=10.0, betaEwald=beta,
+                                name="pair")
+        nb = NbDirect(t)
+        pos = nb.positions_tensor()
+        nb.update_domdec(pos, True)
+        f, _, e = nb.evaluate(pos)
+        torch.cuda.synchronize()
+        d = xyz[0].astype(np.float64) - xyz[1].astype(np.float64)
+        rr = float(np.linalg.norm(d))
+        qq = k * float(np.float32(0.83)) * float(np.float32(-0.61))
+        E = qq * erfc(beta * rr) / rr
+        dEdr = -qq * (erfc(beta * rr) / rr + 2 * beta / sqrt(pi) * exp(-(beta * rr) ** 2)) / rr
+        g0 = dEdr * d / rr                           # dU/dx of atom 0
+        # relative error, with the 2^-32 quantum of the fixed-point sums as floor
+        worst_e = max(worst_e, abs(float(e[0]) - E) / (abs(E) + 1e-3))
+        worst_f = max(worst_f, float(np.abs(f.cpu().numpy()[0] - g0).max()) / (float(np.abs(g0).max()) + 1e-3))
+        nb.close()
+    assert worst_e <= 2e-6, worst_e
+    assert worst_f <= 2e-6, worst_f
