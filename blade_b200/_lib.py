@@ -74,8 +74,8 @@ def lib():
             "bnb_bias": (i, [i, p, p, i, p, p, p, p]),
             "bnb_theta_force_f32": (i, [i, p, p, d, p, p, p, p, p, p]),
             "bnb_bias_f32": (i, [i, p, p, i, p, p, p, p]),
-            "bnb_set_tuning": (i, [p, i, i]),
-            "bnb_get_tuning": (i, [p, p, p]),
+            "bnb_set_tuning": (i, [p, i, i, i]),
+            "bnb_get_tuning": (i, [p, p, p, p]),
             "bnb_autotune": (i, [p, p, p, p, i, p, p]),
             "bnb_set_pairs": (i, [p, i, p, i, p, i]),
             "bnb_compute_nb14": (i, [p, p, p, p, i, p, p]),

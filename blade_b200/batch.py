@@ -315,9 +315,7 @@ class MsldBatch:
         return best.value
 
     def tuning(self):
-        t, c = C.c_int(), C.c_int()
-        _lib.call("bnb_get_tuning", self.nb.h, C.byref(t), C.byref(c))
-        return {"tiles_per_work": t.value, "ctas_per_sm": c.value}
+        return self.nb.tuning()
 
     def check(self):
         st = self.nb.status()

@@ -17,6 +17,7 @@ constexpr int kNumShifts = 14;        // own image + 13 half-shell images
 constexpr int kExclBlk = 16;          // exclusion-partner blocks listed per block
 constexpr int kTilesPerWork = 8;      // default candidate tiles per pair-kernel work item
 constexpr int kMinTilesPerWork = 1;   // smallest setting (sizes the work-item capacity)
+constexpr int kTailItems = 2;         // full-size items' worth of tiles per i block in the tail segment
 constexpr int kMaxTableTypes = 64;    // LJ table kept in shared memory up to 64 types
 constexpr int kMaxLambdaShared = 2048;
 constexpr int kSortCap = 4096;        // column sort in shared memory up to 4096 atoms
@@ -102,6 +103,8 @@ struct Dev {
   // --- static topology (set_topology) -------------------------------------
   int N, R, nTypes, ljCombine, lamTotal;
   int tilesPerWork;        // candidate tiles per work item (tuning knob, 1..32)
+  int tailTiles;           // last candidate tiles of each i block that go to the tail segment
+  int tailTileSize;        // candidate tiles per tail-segment work item
   RepInfo *rep;            // [R]
   int *atomRep;            // [N]
   float *atomQ;            // [N] charge * sqrt(kElectric)
@@ -141,9 +144,11 @@ struct Dev {
   int *candMaskOff;        // [capCand+1]
   uint32_t *masks;         // [capMask*32]
   int *candStart;          // [maxBlocks+1]
-  int *workCountPerBlock;  // [maxBlocks]
+  int *workCountPerBlock;  // [maxBlocks] head-segment items of the block
   int *workOffset;         // [maxBlocks+1]
-  int2 *work;              // [capWork] (iBlock, candidate start)
+  int *workTailCount;      // [maxBlocks] tail-segment items of the block
+  int *workTailOffset;     // [maxBlocks+1]
+  int2 *work;              // [capWork] (iBlock | tiles << 22, candidate start)
   int *scanPartial;        // scratch for multi-CTA scans
   // --- per-step buffers -----------------------------------------------------
   float4 *xyzq;            // [32*maxBlocks]

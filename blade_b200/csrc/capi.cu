@@ -52,6 +52,7 @@ struct bnb_handle {
   int resTiles = 0, resMasks = 0, resWork = 0;
   bool reserveDirty = false;
   int tilesPerWork = bnb::kTilesPerWork, ctasPerSM = 0;  // tuning (bnb_set_tuning / bnb_autotune)
+  int tailItems = bnb::kTailItems;
   int smCount = 0;
   bool counting = false;
   // profiling (bnb_profile)
@@ -202,7 +203,7 @@ int alloc_list(bnb_handle *h) {
          o_cmo = a.take<int>(h->capCand + 1);
   size_t o_masks = a.take<uint32_t>(32 * (size_t)h->capMask);
   size_t o_cs = a.take<int>(MB + 1), o_wcb = a.take<int>(MB), o_wo = a.take<int>(MB + 1),
-         o_work = a.take<int2>(h->capWork);
+         o_work = a.take<int2>(h->capWork), o_wtc = a.take<int>(MB), o_wto = a.take<int>(MB + 1);
   size_t o_part = a.take<int>(4096);
   size_t o_xyzq = a.take<float4>(32 * MB), o_bmin = a.take<float4>(MB), o_bmax = a.take<float4>(MB);
   size_t o_acc = a.take<long long>(3 * 32 * (size_t)MB);
@@ -242,6 +243,8 @@ int alloc_list(bnb_handle *h) {
   d.workCountPerBlock = (int *)(b + o_wcb);
   d.workOffset = (int *)(b + o_wo);
   d.work = (int2 *)(b + o_work);
+  d.workTailCount = (int *)(b + o_wtc);
+  d.workTailOffset = (int *)(b + o_wto);
   d.scanPartial = (int *)(b + o_part);
   d.xyzq = (float4 *)(b + o_xyzq);
   d.bmin = (float4 *)(b + o_bmin);
@@ -632,6 +635,19 @@ int bnb_set_topology(bnb_handle *h, const bnb_nbond *nbonds, const int *typeCoun
   return BNB_OK;
 }
 
+// Tail segment of the work list: the pair kernel's warps take work items in
+// list order, and the last item each warp takes decides when it finishes.
+// Each i block's last tailItems * tilesPerWork candidate tiles therefore form
+// items of a quarter of the full size placed after all the others, so that
+// warps that run out of large items early keep taking small ones while the
+// rest finish.  The split depends on the block's own candidates only: an
+// i atom's force is summed in FP32 over the tiles of one item, so a replica
+// gives the same bits alone and in a batch.
+static void set_tail(bnb_handle *h) {
+  h->d.tailTiles = h->tailItems * h->tilesPerWork;
+  h->d.tailTileSize = std::max(1, h->tilesPerWork / 4);
+}
+
 int bnb_rebuild(bnb_handle *h, const float *position, const float *boxes, void *stream, int flags) {
   if (!h || !boxes || (h->N > 0 && !position)) return BNB_ERR_ARG;
   if (!h->topo) return BNB_ERR_STATE;
@@ -667,6 +683,7 @@ int bnb_rebuild(bnb_handle *h, const float *position, const float *boxes, void *
   const float rcull = h->p.rCut + h->p.cullPad;
   const float rcull2 = rcull * rcull;
   h->d.tilesPerWork = h->tilesPerWork;
+  set_tail(h);
   for (int attempt = 0; attempt < 12; attempt++) {
     const bool rec = h->prof && h->rebN < kProfSlots;
     if (rec) cudaEventRecord(h->rebEv[2 * h->rebN], s);
@@ -806,24 +823,29 @@ int bnb_profile_read(bnb_handle *h, double *pairMs, int *pairLaunches, double *r
   return BNB_OK;
 }
 
-int bnb_set_tuning(bnb_handle *h, int tilesPerWork, int ctasPerSM) {
-  if (!h || tilesPerWork < bnb::kMinTilesPerWork || tilesPerWork > 32 || ctasPerSM < 0 || ctasPerSM > 8)
+int bnb_set_tuning(bnb_handle *h, int tilesPerWork, int ctasPerSM, int tailItems) {
+  if (!h || tilesPerWork < bnb::kMinTilesPerWork || tilesPerWork > 32 || ctasPerSM < 0 || ctasPerSM > 8 ||
+      tailItems < 0 || tailItems > 8)
     return BNB_ERR_ARG;
-  if (tilesPerWork != h->tilesPerWork) h->listBuilt = false;  // work items must be rebuilt
+  // work items must be rebuilt
+  if (tilesPerWork != h->tilesPerWork || tailItems != h->tailItems) h->listBuilt = false;
   h->tilesPerWork = tilesPerWork;
   h->ctasPerSM = ctasPerSM;
+  h->tailItems = tailItems;
   return BNB_OK;
 }
 
-int bnb_get_tuning(bnb_handle *h, int *tilesPerWork, int *ctasPerSM) {
+int bnb_get_tuning(bnb_handle *h, int *tilesPerWork, int *ctasPerSM, int *tailItems) {
   if (!h) return BNB_ERR_ARG;
   if (tilesPerWork) *tilesPerWork = h->tilesPerWork;
   if (ctasPerSM) *ctasPerSM = h->ctasPerSM;
+  if (tailItems) *tailItems = h->tailItems;
   return BNB_OK;
 }
 
-// Tries tiles-per-work-item x CTAs-per-SM settings on the caller's system and
-// keeps the fastest pair-kernel time (CUDA events, median of `reps`).
+// Tries tiles-per-work-item x CTAs-per-SM x tail settings on the caller's
+// system and keeps the fastest pair-kernel time (CUDA events, median of
+// `reps`).
 int bnb_autotune(bnb_handle *h, const float *position, const float *lambda, const float *boxes,
                  int reps, void *stream, float *bestMs) {
   if (!h || !boxes || (h->N > 0 && !position) || reps < 1) return BNB_ERR_ARG;
@@ -831,16 +853,18 @@ int bnb_autotune(bnb_handle *h, const float *position, const float *lambda, cons
   cudaStream_t s = (cudaStream_t)stream;
   static const int kTiles[] = {1, 2, 4, 8, 16, 32};
   static const int kCtas[] = {0, 2, 3};
+  static const int kTails[] = {bnb::kTailItems, 0};
   bnb_outputs none;
   memset(&none, 0, sizeof(none));
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   float best = 1e30f;
-  int bt = h->tilesPerWork, bc = h->ctasPerSM;
+  int bt = h->tilesPerWork, bc = h->ctasPerSM, bl = h->tailItems;
+  for (int l : kTails)
   for (int t : kTiles) {
     for (int c : kCtas) {
-      int rc = bnb_set_tuning(h, t, c);
+      int rc = bnb_set_tuning(h, t, c, l);
       if (!rc) rc = bnb_rebuild(h, position, boxes, stream, 0);
       if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
       std::vector<float> ms;
@@ -856,12 +880,12 @@ int bnb_autotune(bnb_handle *h, const float *position, const float *lambda, cons
       }
       std::sort(ms.begin(), ms.end());
       float med = ms[ms.size() / 2];
-      if (med < best) { best = med; bt = t; bc = c; }
+      if (med < best) { best = med; bt = t; bc = c; bl = l; }
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  int rc = bnb_set_tuning(h, bt, bc);
+  int rc = bnb_set_tuning(h, bt, bc, bl);
   if (!rc) rc = bnb_rebuild(h, position, boxes, stream, 0);
   if (bestMs) *bestMs = best;
   return rc;

@@ -586,10 +586,10 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
   w = __shfl_sync(kFull, w, 0);
   while (w < nWork) {
     const int2 wk = d.work[w];
-    const int iBlock = wk.x;
+    const int iBlock = wk.x & 0x3FFFFF;
     const int c0 = wk.y;
     int c1 = d.candStart[iBlock + 1];
-    c1 = c1 < c0 + d.tilesPerWork ? c1 : c0 + d.tilesPerWork;
+    c1 = c1 < c0 + (wk.x >> 22) ? c1 : c0 + (wk.x >> 22);
     const int islot = 32 * iBlock + lane;
     float4 xi = d.xyzq[islot];
     const bool iValid = d.slotAtom[islot] >= 0;

@@ -218,21 +218,28 @@ class NbDirect:
         return l64, e64
 
     # -- tuning -------------------------------------------------------------------
-    def set_tuning(self, tiles_per_work: int, ctas_per_sm: int = 0):
-        """bnb_set_tuning: candidate tiles per work item (1..32) and resident CTAs
-        per SM of the persistent pair kernel (0 = occupancy); the next rebuild applies it."""
-        _lib.call("bnb_set_tuning", self.h, int(tiles_per_work), int(ctas_per_sm))
+    def set_tuning(self, tiles_per_work: int, ctas_per_sm: int = 0, tail_items: int = 2):
+        """bnb_set_tuning: candidate tiles per work item (1..32), resident CTAs
+        per SM of the persistent pair kernel (0 = occupancy) and the work-list
+        tail (0..8 full items' worth of each block's tiles in quarter-size
+        items at the end); the next rebuild applies it."""
+        _lib.call("bnb_set_tuning", self.h, int(tiles_per_work), int(ctas_per_sm), int(tail_items))
+
+    def tuning(self) -> dict:
+        """bnb_get_tuning."""
+        t, c, l = C.c_int(), C.c_int(), C.c_int()
+        _lib.call("bnb_get_tuning", self.h, C.byref(t), C.byref(c), C.byref(l))
+        return {"tiles_per_work": t.value, "ctas_per_sm": c.value, "tail_items": l.value}
 
     def autotune(self, positions, lambdas=None, reps: int = 5, stream=None) -> dict:
-        """bnb_autotune: tries tiles per work item x CTAs per SM on this system,
-        keeps the fastest (median of ``reps``), rebuilds the list; returns the choice."""
+        """bnb_autotune: tries tiles per work item x CTAs per SM x tail on this
+        system, keeps the fastest (median of ``reps``), rebuilds the list;
+        returns the choice."""
         best = C.c_float()
         b = np.ascontiguousarray(self.boxes, np.float32)
         _lib.call("bnb_autotune", self.h, _ptr(positions), _ptr(lambdas), b.ctypes.data_as(C.c_void_p), int(reps),
                   _stream(stream), C.byref(best))
-        t, c = C.c_int(), C.c_int()
-        _lib.call("bnb_get_tuning", self.h, C.byref(t), C.byref(c))
-        return {"tiles_per_work": t.value, "ctas_per_sm": c.value, "best_ms": best.value}
+        return dict(self.tuning(), best_ms=best.value)
 
     # -- conveniences ------------------------------------------------------------
     def positions_tensor(self, xyz_list=None):

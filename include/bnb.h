@@ -377,12 +377,18 @@ int bnb_bias_f32(int blockCount, const float *lambda, const float *fixedBias,
 
 /* ---- batched stepping: tuning and integrator ----------------------------- */
 /*
- * Tuning knobs of the pair kernel: candidate tiles per work item (1..32) and
- * CTAs per SM of the persistent grid (0 = as many as fit).  A changed tile
- * count takes effect at the next bnb_rebuild.  No reference counterpart.
+ * Tuning knobs of the pair kernel: candidate tiles per work item (1..32),
+ * CTAs per SM of the persistent grid (0 = as many as fit) and the tail of the
+ * work list (0..8): the last tailItems * tilesPerWork candidate tiles of every
+ * i block become items of a quarter of the size, taken after all others, so
+ * that the persistent warps finish close together (0 = no tail; default 2).
+ * A changed tile count or tail takes effect at the next bnb_rebuild.  The
+ * split of each block's tiles depends on that block alone, so a replica gives
+ * the same bits alone and in a batch at equal settings.  No reference
+ * counterpart.
  */
-int bnb_set_tuning(bnb_handle *h, int tilesPerWork, int ctasPerSM);
-int bnb_get_tuning(bnb_handle *h, int *tilesPerWork, int *ctasPerSM);
+int bnb_set_tuning(bnb_handle *h, int tilesPerWork, int ctasPerSM, int tailItems);
+int bnb_get_tuning(bnb_handle *h, int *tilesPerWork, int *ctasPerSM, int *tailItems);
 /*
  * Adds one sampling step of lambda (FP64, [blockCount]) to histograms, the
  * statistics adaptive landscape flattening takes from the .lmd lambda
@@ -398,9 +404,10 @@ int bnb_lambda_histogram(int blockCount, const double *lambda, const uint8_t *bl
 
 /*
  * Autotuner: times every (tiles per work item in {1,2,4,8,16,32}) x (CTAs per
- * SM in {auto,2,3}) setting on the caller's coordinates (median of `reps`
- * evaluations, CUDA events), keeps the fastest and rebuilds the list with it.
- * Synchronises.  bestMs: the kept setting's pair-evaluation time.
+ * SM in {auto,2,3}) x (tail in {2,0}) setting on the caller's coordinates
+ * (median of `reps` evaluations, CUDA events), keeps the fastest and rebuilds
+ * the list with it.  Synchronises.  bestMs: the kept setting's
+ * pair-evaluation time.
  */
 int bnb_autotune(bnb_handle *h, const float *position, const float *lambda,
                  const float *boxes, int reps, void *stream, float *bestMs);

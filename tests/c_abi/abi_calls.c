@@ -43,8 +43,9 @@ static int argument_checks(void) {
   CHECK(bnb_compute(h, NULL, NULL, box, 1, &out, NULL), BNB_ERR_STATE);
   CHECK(bnb_set_pme(h, 5, 1.0f, NULL, box), BNB_ERR_ARG);           /* orders 4, 6, 8 */
   CHECK(bnb_set_pme(h, 6, 1.0f, NULL, box), BNB_ERR_STATE);
-  CHECK(bnb_set_tuning(h, 0, 0), BNB_ERR_ARG);                       /* 1..32 tiles per work item */
-  CHECK(bnb_set_tuning(h, 4, 3), BNB_OK);
+  CHECK(bnb_set_tuning(h, 0, 0, 2), BNB_ERR_ARG);                    /* 1..32 tiles per work item */
+  CHECK(bnb_set_tuning(h, 4, 3, 9), BNB_ERR_ARG);                    /* tail 0..8 */
+  CHECK(bnb_set_tuning(h, 4, 3, 0), BNB_OK);
   CHECK(bnb_destroy(h), BNB_OK);
   memset(&empty, 0, sizeof(empty));
   CHECK(bnb_holonomic_position(&empty, x, x, NULL, x, 0.02, 1e-10, 10, NULL, NULL, NULL), BNB_OK);

@@ -67,6 +67,7 @@ def test_autotune_keeps_results_valid(cuda, reps):
     B = MsldBatch(reps, tune=True)
     t = B.tuning()
     assert t["tiles_per_work"] in (1, 2, 4, 8, 16, 32) and t["ctas_per_sm"] in (0, 2, 3)
+    assert t["tail_items"] in (0, 2)
     B.run_eager(10)
     assert B.check() == (0, 0)
     B.close()
