@@ -412,17 +412,18 @@ __device__ __forceinline__ void plain_loop(JRegs<COMBINE, ALCH> &J, const float4
 // ---------------------------------------------------------------------------
 // Streamed tiles.  The compacted j atoms of a work item's tiles that need no
 // exclusion mask and no MSLD scaling are queued in shared memory as entries
-// (j slot | shift code << 27) and evaluated in chunks of up to 64: every lane
-// keeps its i atom and holds two queued j atoms, A = entry cl and B = entry
-// gj + cl of its group of gj lanes (gj = 32, 16, 8 or 4 for chunks of more
-// than 32, 16, 8 or up to 8 entries; smaller groups are replicated), and the
-// pair math of A and B runs in packed FP32x2 instructions.  After gj rotation
-// steps each group lane holds the group's partial forces of its own two
-// entries; the groups are summed by xor shuffles and group 0 adds them to the
-// fixed-point accumulators, one addition per queued j atom.  A chunk costs its
-// entry count rounded up to an even number of gj-lane rotations, so a tile
-// contributes exactly its compacted j atoms and only the last chunk of a work
-// item is padded.
+// (j slot | shift code << 27) and evaluated in rounds of up to 32.  For these
+// rounds lane l holds two i atoms of the block, A = l mod 16 and B = A + 16,
+// so each half of the warp covers the whole i block, and one queued j atom:
+// with rounds of width gw (16, 8 or 4) half h takes entries h gw .. h gw +
+// gw - 1, one per lane of each of its 16 / gw groups of gw lanes.  The j atom
+// meets its lane's two i atoms in packed FP32x2 instructions and rotates
+// through the group with its force accumulator, so a rotation step moves one
+// j atom for two pairs.  After gw steps the groups of a half are summed by
+// xor shuffles and group 0 adds each entry's force to the fixed-point
+// accumulators, one addition per queued j atom.  A round costs gw steps for
+// up to 2 gw entries, so a tile contributes exactly its compacted j atoms and
+// only the last round of a work item is padded.
 // ---------------------------------------------------------------------------
 template <bool COMBINE>
 __device__ __forceinline__ void stream_load(const Dev &d, int e, const float4 *shifts, float &x, float &y,
@@ -446,93 +447,93 @@ __device__ __forceinline__ void stream_load(const Dev &d, int e, const float4 *s
   }
 }
 
+// The two i atoms of a lane in the streamed rounds: position and scaled
+// charge of A (.x) and B (.y), LJ parameters (combine mode) or table rows.
+struct IPair {
+  float2 x, y, z, q;
+  float2 e6, R;   // combine mode: (sqrt(12 eps), Rmin/2) of A and B
+  int rowA, rowB; // table mode: type * nTypes of A and B
+};
+
 template <int ELEC, int VDW, bool ENERGY, bool COMBINE>
-__device__ __forceinline__ void stream_chunk(const Dev &d, const PairConst &pc, const float2 *sLJ, const int *sS,
-                                             int C, int lane, float4 xi, int rowI, float2 ljI, const float4 *shifts,
+__device__ __forceinline__ void stream_round(const Dev &d, const PairConst &pc, const float2 *sLJ, const int *sS,
+                                             int C, int lane, const IPair &I, const float4 *shifts,
                                              float2 &fix2, float2 &fiy2, float2 &fiz2, long long &ei,
                                              unsigned long long &pairs, int count) {
-  const int gj = C > 32 ? 32 : (C > 16 ? 16 : (C > 8 ? 8 : 4));
-  const int cl = lane & (gj - 1);
-  const int eA = cl < C ? sS[cl] : -1;
-  const int eB = gj + cl < C ? sS[gj + cl] : -1;
-  float2 jx, jy, jz, jq, jex = f2(0.f), jer = f2(0.f);
-  int tA, tB;
-  stream_load<COMBINE>(d, eA, shifts, jx.x, jy.x, jz.x, jq.x, tA, jex.x, jer.x);
-  stream_load<COMBINE>(d, eB, shifts, jx.y, jy.y, jz.y, jq.y, tB, jex.y, jer.y);
-  float2 jfx = f2(0.f), jfy = f2(0.f), jfz = f2(0.f);
-  const float2 xi2 = f2(xi.x), yi2 = f2(xi.y), zi2 = f2(xi.z), qi2 = f2(xi.w);
-  const float2 m1 = f2(-1.f);
-  const int rot = lane + 1;
+  const int gw = C > 16 ? 16 : (C > 8 ? 8 : 4);
+  const int cl = lane & (gw - 1);
+  const int eIdx = (lane >> 4) * gw + cl;
+  const int e = eIdx < C ? sS[eIdx] : -1;
+  float jx, jy, jz, jq, jex = 0.f, jer = 0.f;
+  int tj;
+  stream_load<COMBINE>(d, e, shifts, jx, jy, jz, jq, tj, jex, jer);
+  float jfx = 0.f, jfy = 0.f, jfz = 0.f;
 #pragma unroll 2
-  for (int k = 0; k < gj; k++) {
-    const float2 dx = fma2(jx, m1, xi2), dy = fma2(jy, m1, yi2), dz = fma2(jz, m1, zi2);
+  for (int k = 0; k < gw; k++) {
+    const float2 dx = make_float2(I.x.x - jx, I.x.y - jx);
+    const float2 dy = make_float2(I.y.x - jy, I.y.y - jy);
+    const float2 dz = make_float2(I.z.x - jz, I.z.y - jz);
     const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
     const bool actA = r2.x < pc.rc2, actB = r2.y < pc.rc2;
+    const float2 qq = make_float2(I.q.x * jq, I.q.y * jq);
     float2 fs, E = f2(0.f);
     if (ELEC == 1 && VDW == 0) {
       float2 lj0, lj1;
       if (COMBINE) {
-        lj0 = mul2(f2(ljI.x), jex);
-        lj1 = add2(f2(ljI.y), jer);
+        lj0 = make_float2(I.e6.x * jex, I.e6.y * jex);
+        lj1 = make_float2(I.R.x + jer, I.R.y + jer);
       } else {
-        const float2 vA = sLJ[rowI + tA], vB = sLJ[rowI + tB];
+        const float2 vA = sLJ[I.rowA + tj], vB = sLJ[I.rowB + tj];
         lj0 = make_float2(vA.x, vB.x);
         lj1 = make_float2(vA.y, vB.y);
       }
-      fs = pme_vfsw_pair2<ENERGY, COMBINE>(pc, r2, mul2(qi2, jq), lj0, lj1, E);
+      fs = pme_vfsw_pair2<ENERGY, COMBINE>(pc, r2, qq, lj0, lj1, E);
     } else {
-      fs.x = plain_pair<ELEC, VDW, ENERGY, COMBINE>(pc, r2.x, xi.w * jq.x, sLJ, rowI, tA, ljI,
-                                                    make_float2(jex.x, jer.x), E.x);
-      fs.y = plain_pair<ELEC, VDW, ENERGY, COMBINE>(pc, r2.y, xi.w * jq.y, sLJ, rowI, tB, ljI,
-                                                    make_float2(jex.y, jer.y), E.y);
+      fs.x = plain_pair<ELEC, VDW, ENERGY, COMBINE>(pc, r2.x, qq.x, sLJ, I.rowA, tj,
+                                                    make_float2(I.e6.x, I.R.x), make_float2(jex, jer), E.x);
+      fs.y = plain_pair<ELEC, VDW, ENERGY, COMBINE>(pc, r2.y, qq.y, sLJ, I.rowB, tj,
+                                                    make_float2(I.e6.y, I.R.y), make_float2(jex, jer), E.y);
     }
     fs = sel2(actA, actB, fs, f2(0.f));
     fix2 = fma2(fs, dx, fix2);
     fiy2 = fma2(fs, dy, fiy2);
     fiz2 = fma2(fs, dz, fiz2);
-    jfx = fma2(fs, dx, jfx);  // the j atoms' forces with the sign of the i side, negated below
-    jfy = fma2(fs, dy, jfy);
-    jfz = fma2(fs, dz, jfz);
+    // the j atom's force with the sign of the i side, negated below
+    jfx = fmaf(fs.x, dx.x, fmaf(fs.y, dx.y, jfx));
+    jfy = fmaf(fs.x, dy.x, fmaf(fs.y, dy.y, jfy));
+    jfz = fmaf(fs.x, dz.x, fmaf(fs.y, dz.y, jfz));
     if (ENERGY) {
       if (actA) ei += to_fix(E.x);
       if (actB) ei += to_fix(E.y);
       if (count) pairs += (unsigned long long)actA + (unsigned long long)actB;
     }
-    jx.x = __shfl_sync(kFull, jx.x, rot, gj); jx.y = __shfl_sync(kFull, jx.y, rot, gj);
-    jy.x = __shfl_sync(kFull, jy.x, rot, gj); jy.y = __shfl_sync(kFull, jy.y, rot, gj);
-    jz.x = __shfl_sync(kFull, jz.x, rot, gj); jz.y = __shfl_sync(kFull, jz.y, rot, gj);
-    jq.x = __shfl_sync(kFull, jq.x, rot, gj); jq.y = __shfl_sync(kFull, jq.y, rot, gj);
+    jx = __shfl_sync(kFull, jx, lane + 1, gw);
+    jy = __shfl_sync(kFull, jy, lane + 1, gw);
+    jz = __shfl_sync(kFull, jz, lane + 1, gw);
+    jq = __shfl_sync(kFull, jq, lane + 1, gw);
     if (COMBINE) {
-      jex.x = __shfl_sync(kFull, jex.x, rot, gj); jex.y = __shfl_sync(kFull, jex.y, rot, gj);
-      jer.x = __shfl_sync(kFull, jer.x, rot, gj); jer.y = __shfl_sync(kFull, jer.y, rot, gj);
+      jex = __shfl_sync(kFull, jex, lane + 1, gw);
+      jer = __shfl_sync(kFull, jer, lane + 1, gw);
     } else {
-      tA = __shfl_sync(kFull, tA, rot, gj); tB = __shfl_sync(kFull, tB, rot, gj);
+      tj = __shfl_sync(kFull, tj, lane + 1, gw);
     }
-    jfx.x = __shfl_sync(kFull, jfx.x, rot, gj); jfx.y = __shfl_sync(kFull, jfx.y, rot, gj);
-    jfy.x = __shfl_sync(kFull, jfy.x, rot, gj); jfy.y = __shfl_sync(kFull, jfy.y, rot, gj);
-    jfz.x = __shfl_sync(kFull, jfz.x, rot, gj); jfz.y = __shfl_sync(kFull, jfz.y, rot, gj);
+    jfx = __shfl_sync(kFull, jfx, lane + 1, gw);
+    jfy = __shfl_sync(kFull, jfy, lane + 1, gw);
+    jfz = __shfl_sync(kFull, jfz, lane + 1, gw);
   }
-  for (int o = 16; o >= gj; o >>= 1) {
-    jfx.x += __shfl_xor_sync(kFull, jfx.x, o); jfx.y += __shfl_xor_sync(kFull, jfx.y, o);
-    jfy.x += __shfl_xor_sync(kFull, jfy.x, o); jfy.y += __shfl_xor_sync(kFull, jfy.y, o);
-    jfz.x += __shfl_xor_sync(kFull, jfz.x, o); jfz.y += __shfl_xor_sync(kFull, jfz.y, o);
+  // the groups of a half hold the same entries: sum them (not across halves)
+  for (int o = 8; o >= gw; o >>= 1) {
+    jfx += __shfl_xor_sync(kFull, jfx, o);
+    jfy += __shfl_xor_sync(kFull, jfy, o);
+    jfz += __shfl_xor_sync(kFull, jfz, o);
   }
-  if (lane < gj) {
+  if ((lane & 15) < gw && e >= 0 && (jfx != 0.f || jfy != 0.f || jfz != 0.f)) {
     const int S = 32 * d.maxBlocks;
-    if (eA >= 0 && (jfx.x != 0.f || jfy.x != 0.f || jfz.x != 0.f)) {
-      const int js = eA & 0x7FFFFFF;
-      red_add(&d.accF[js], to_fix(-jfx.x));
-      red_add(&d.accF[S + js], to_fix(-jfy.x));
-      red_add(&d.accF[2 * S + js], to_fix(-jfz.x));
-      if (!(isfinite(jfx.x) && isfinite(jfy.x) && isfinite(jfz.x))) atomicOr(&d.ctr->status, kStatusNonFinite);
-    }
-    if (eB >= 0 && (jfx.y != 0.f || jfy.y != 0.f || jfz.y != 0.f)) {
-      const int js = eB & 0x7FFFFFF;
-      red_add(&d.accF[js], to_fix(-jfx.y));
-      red_add(&d.accF[S + js], to_fix(-jfy.y));
-      red_add(&d.accF[2 * S + js], to_fix(-jfz.y));
-      if (!(isfinite(jfx.y) && isfinite(jfy.y) && isfinite(jfz.y))) atomicOr(&d.ctr->status, kStatusNonFinite);
-    }
+    const int js = e & 0x7FFFFFF;
+    red_add(&d.accF[js], to_fix(-jfx));
+    red_add(&d.accF[S + js], to_fix(-jfy));
+    red_add(&d.accF[2 * S + js], to_fix(-jfz));
+    if (!(isfinite(jfx) && isfinite(jfy) && isfinite(jfz))) atomicOr(&d.ctr->status, kStatusNonFinite);
   }
 }
 
@@ -615,7 +616,25 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
     unsigned act = __ballot_sync(kFull, hit);
 
     float fix = 0.f, fiy = 0.f, fiz = 0.f, fli = 0.f;
-    float2 fix2 = f2(0.f), fiy2 = f2(0.f), fiz2 = f2(0.f);  // i forces of the streamed pairs (A, B)
+    // i atoms A = lane mod 16 and B = A + 16 of the streamed rounds, their forces
+    IPair ip;
+    {
+      const int a = lane & 15;
+      ip.x = make_float2(__shfl_sync(kFull, xi.x, a), __shfl_sync(kFull, xi.x, a + 16));
+      ip.y = make_float2(__shfl_sync(kFull, xi.y, a), __shfl_sync(kFull, xi.y, a + 16));
+      ip.z = make_float2(__shfl_sync(kFull, xi.z, a), __shfl_sync(kFull, xi.z, a + 16));
+      ip.q = make_float2(__shfl_sync(kFull, xi.w, a), __shfl_sync(kFull, xi.w, a + 16));
+      if (COMBINE) {
+        ip.e6 = make_float2(__shfl_sync(kFull, ljI.x, a), __shfl_sync(kFull, ljI.x, a + 16));
+        ip.R = make_float2(__shfl_sync(kFull, ljI.y, a), __shfl_sync(kFull, ljI.y, a + 16));
+        ip.rowA = ip.rowB = 0;
+      } else {
+        ip.e6 = ip.R = f2(0.f);
+        ip.rowA = __shfl_sync(kFull, rowI, a);
+        ip.rowB = __shfl_sync(kFull, rowI, a + 16);
+      }
+    }
+    float2 fix2 = f2(0.f), fiy2 = f2(0.f), fiz2 = f2(0.f);
     int nS = 0;        // entries queued in sStream[warp]
     long long ei = 0;  // fixed-point energy of this lane's pairs
     // The loads of each tile are issued one tile ahead, so their latency
@@ -661,11 +680,11 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
         if (jin) sStream[warp][nS + rank] = jslot | (code << 27);
         nS += nj;
         __syncwarp();
-        if (nS >= 64) {
-          stream_chunk<ELEC, VDW, ENERGY, COMBINE>(d, pc, sLJ, sStream[warp], 64, lane, xi, rowI, ljI, shifts,
-                                                   fix2, fiy2, fiz2, ei, pairs, A.count);
-          const int rest = nS - 64;  // < 32
-          const int carry = lane < rest ? sStream[warp][64 + lane] : 0;
+        if (nS >= 32) {
+          stream_round<ELEC, VDW, ENERGY, COMBINE>(d, pc, sLJ, sStream[warp], 32, lane, ip, shifts, fix2, fiy2,
+                                                   fiz2, ei, pairs, A.count);
+          const int rest = nS - 32;  // < 32
+          const int carry = lane < rest ? sStream[warp][32 + lane] : 0;
           __syncwarp();
           if (lane < rest) sStream[warp][lane] = carry;
           __syncwarp();
@@ -800,20 +819,25 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
         atomicAdd(reinterpret_cast<unsigned long long *>(&sAccL[bj0 & 0xFFFF]),
                   static_cast<unsigned long long>(to_fix(ofl)));
     }
-    // the rest of the queue (< 64 entries) in chunks of 64, 32, 16 or 8,
-    // whichever pads least: e.g. 40 entries as 32 + 8 (20 steps, not 32)
+    // the rest of the queue (< 32 entries) in rounds of 32, 16 or 8 entries,
+    // whichever pads least: e.g. 20 entries as 16 + 8 (12 steps, not 16)
     for (int off = 0; off < nS;) {
       const int rem = nS - off;
-      const int cap = rem > 48 ? 64 : (rem > 24 ? 32 : (rem > 12 ? 16 : 8));
+      const int cap = rem > 24 ? 32 : (rem > 12 ? 16 : 8);
       const int cnt = rem < cap ? rem : cap;
-      stream_chunk<ELEC, VDW, ENERGY, COMBINE>(d, pc, sLJ, sStream[warp] + off, cnt, lane, xi, rowI, ljI, shifts,
-                                               fix2, fiy2, fiz2, ei, pairs, A.count);
+      stream_round<ELEC, VDW, ENERGY, COMBINE>(d, pc, sLJ, sStream[warp] + off, cnt, lane, ip, shifts, fix2, fiy2,
+                                               fiz2, ei, pairs, A.count);
       off += cnt;
     }
     __syncwarp();  // sStream is rewritten by the next work item
-    fix += fix2.x + fix2.y;
-    fiy += fiy2.x + fiy2.y;
-    fiz += fiz2.x + fiz2.y;
+    // the two halves hold the same i atoms: after the sum, lane l < 16 has
+    // atom l in .x and lane l >= 16 atom l in .y
+    fix2.x += __shfl_xor_sync(kFull, fix2.x, 16); fix2.y += __shfl_xor_sync(kFull, fix2.y, 16);
+    fiy2.x += __shfl_xor_sync(kFull, fiy2.x, 16); fiy2.y += __shfl_xor_sync(kFull, fiy2.y, 16);
+    fiz2.x += __shfl_xor_sync(kFull, fiz2.x, 16); fiz2.y += __shfl_xor_sync(kFull, fiz2.y, 16);
+    fix += lane < 16 ? fix2.x : fix2.y;
+    fiy += lane < 16 ? fiy2.x : fiy2.y;
+    fiz += lane < 16 ? fiz2.x : fiz2.y;
     if (iValid && (fix != 0.f || fiy != 0.f || fiz != 0.f)) {
       red_add(&d.accF[islot], to_fix(fix));
       red_add(&d.accF[S + islot], to_fix(fiy));
