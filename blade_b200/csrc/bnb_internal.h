@@ -10,6 +10,7 @@
 #include <stdint.h>
 
 #include "bnb.h"
+#include "work_split.h"
 
 namespace bnb {
 
@@ -17,7 +18,7 @@ constexpr int kNumShifts = 14;        // own image + 13 half-shell images
 constexpr int kExclBlk = 16;          // exclusion-partner blocks listed per block
 constexpr int kTilesPerWork = 8;      // default candidate tiles per pair-kernel work item
 constexpr int kMinTilesPerWork = 1;   // smallest setting (sizes the work-item capacity)
-constexpr int kTailItems = 2;         // full-size items' worth of tiles per i block in the tail segment
+constexpr int kTailItems = 2;         // full-size items' worth of tiles per i block in the tail levels
 constexpr int kMaxTableTypes = 64;    // LJ table kept in shared memory up to 64 types
 constexpr int kMaxLambdaShared = 2048;
 constexpr int kSortCap = 4096;        // column sort in shared memory up to 4096 atoms
@@ -97,14 +98,15 @@ struct Counters {
   int workNext;            // dynamic work-item counter of the pair kernel
   int pad[2];
   unsigned long long pairCount;
+  int levelCount[kWorkLevels];  // work items per level of the work list (rebuild)
+  int levelFill[kWorkLevels];   // items written per level (rebuild)
 };
 
 struct Dev {
   // --- static topology (set_topology) -------------------------------------
   int N, R, nTypes, ljCombine, lamTotal;
   int tilesPerWork;        // candidate tiles per work item (tuning knob, 1..32)
-  int tailTiles;           // last candidate tiles of each i block that go to the tail segment
-  int tailTileSize;        // candidate tiles per tail-segment work item
+  int tailTiles;           // last candidate tiles of each i block that go to the tail levels
   RepInfo *rep;            // [R]
   int *atomRep;            // [N]
   float *atomQ;            // [N] charge * sqrt(kElectric)
@@ -144,10 +146,6 @@ struct Dev {
   int *candMaskOff;        // [capCand+1]
   uint32_t *masks;         // [capMask*32]
   int *candStart;          // [maxBlocks+1]
-  int *workCountPerBlock;  // [maxBlocks] head-segment items of the block
-  int *workOffset;         // [maxBlocks+1]
-  int *workTailCount;      // [maxBlocks] tail-segment items of the block
-  int *workTailOffset;     // [maxBlocks+1]
   int2 *work;              // [capWork] (iBlock | tiles << 22, candidate start)
   int *scanPartial;        // scratch for multi-CTA scans
   // --- per-step buffers -----------------------------------------------------

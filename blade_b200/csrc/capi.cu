@@ -202,8 +202,7 @@ int alloc_list(bnb_handle *h) {
   size_t o_cand = a.take<int4>(h->capCand), o_cflag = a.take<int>(h->capCand),
          o_cmo = a.take<int>(h->capCand + 1);
   size_t o_masks = a.take<uint32_t>(32 * (size_t)h->capMask);
-  size_t o_cs = a.take<int>(MB + 1), o_wcb = a.take<int>(MB), o_wo = a.take<int>(MB + 1),
-         o_work = a.take<int2>(h->capWork), o_wtc = a.take<int>(MB), o_wto = a.take<int>(MB + 1);
+  size_t o_cs = a.take<int>(MB + 1), o_work = a.take<int2>(h->capWork);
   size_t o_part = a.take<int>(4096);
   size_t o_xyzq = a.take<float4>(32 * MB), o_bmin = a.take<float4>(MB), o_bmax = a.take<float4>(MB);
   size_t o_acc = a.take<long long>(3 * 32 * (size_t)MB);
@@ -240,11 +239,7 @@ int alloc_list(bnb_handle *h) {
   d.candMaskOff = (int *)(b + o_cmo);
   d.masks = (uint32_t *)(b + o_masks);
   d.candStart = (int *)(b + o_cs);
-  d.workCountPerBlock = (int *)(b + o_wcb);
-  d.workOffset = (int *)(b + o_wo);
   d.work = (int2 *)(b + o_work);
-  d.workTailCount = (int *)(b + o_wtc);
-  d.workTailOffset = (int *)(b + o_wto);
   d.scanPartial = (int *)(b + o_part);
   d.xyzq = (float4 *)(b + o_xyzq);
   d.bmin = (float4 *)(b + o_bmin);
@@ -635,17 +630,16 @@ int bnb_set_topology(bnb_handle *h, const bnb_nbond *nbonds, const int *typeCoun
   return BNB_OK;
 }
 
-// Tail segment of the work list: the pair kernel's warps take work items in
-// list order, and the last item each warp takes decides when it finishes.
-// Each i block's last tailItems * tilesPerWork candidate tiles therefore form
-// items of a quarter of the full size placed after all the others, so that
-// warps that run out of large items early keep taking small ones while the
-// rest finish.  The split depends on the block's own candidates only: an
-// i atom's force is summed in FP32 over the tiles of one item, so a replica
-// gives the same bits alone and in a batch.
+// Tail of the work list: the pair kernel's warps take work items in list
+// order, and the last item each warp takes decides when it finishes.  Each
+// i block's last tailItems * tilesPerWork candidate tiles therefore form
+// items of halving size (bnb::work_split) placed after all the full-size
+// items, smallest last, so that warps that run out of large items early keep
+// taking small ones while the rest finish.  The split depends on the block's
+// own candidates only: an i atom's force is summed in FP32 over the tiles of
+// one item, so a replica gives the same bits alone and in a batch.
 static void set_tail(bnb_handle *h) {
   h->d.tailTiles = h->tailItems * h->tilesPerWork;
-  h->d.tailTileSize = std::max(1, h->tilesPerWork / 4);
 }
 
 int bnb_rebuild(bnb_handle *h, const float *position, const float *boxes, void *stream, int flags) {

@@ -292,6 +292,10 @@ __global__ void k_colscan(Dev d, const int *__restrict__ colRep) {
     d.blockBounds[B] = carryA;
     d.ctr->blockCount = B;
   }
+  if (threadIdx.x < kWorkLevels) {  // the work list of this rebuild is counted afresh
+    d.ctr->levelCount[threadIdx.x] = 0;
+    d.ctr->levelFill[threadIdx.x] = 0;
+  }
   __syncthreads();
   for (int r = threadIdx.x; r <= d.R; r += blockDim.x) {
     int b = r < d.R ? d.colStartBlock[d.rep[r].colStart] : d.colStartBlock[nc];
@@ -461,10 +465,6 @@ __global__ void k_cull(Dev d, float rcull2) {
     int iBlock = gw / kNumShifts, code = gw - iBlock * kNumShifts;
     if (iBlock >= B) {
       if (!kWrite && lane == 0) d.cullCount[gw] = 0;
-      if (kWrite && lane == 0 && code == 0) {
-        d.workCountPerBlock[iBlock] = 0;
-        d.workTailCount[iBlock] = 0;
-      }
       continue;
     }
     int r = d.blockRep[iBlock];
@@ -528,12 +528,10 @@ __global__ void k_cull(Dev d, float rcull2) {
       c0 = c0 < d.capCand ? c0 : d.capCand;
       c1 = c1 < d.capCand ? c1 : d.capCand;
       d.candStart[iBlock] = c0;
-      // the block's last tailTiles candidates go to the tail segment of the
-      // work list in items of tailTileSize, the rest to the head segment in
-      // items of tilesPerWork
-      const int nc = c1 - c0, nt = nc < d.tailTiles ? nc : d.tailTiles;
-      d.workCountPerBlock[iBlock] = (nc - nt + d.tilesPerWork - 1) / d.tilesPerWork;
-      d.workTailCount[iBlock] = (nt + d.tailTileSize - 1) / d.tailTileSize;
+      int tiles[kWorkLevels], items[kWorkLevels];
+      const int L = work_split(c1 - c0, d.tilesPerWork, d.tailTiles, tiles, items);
+      for (int l = 0; l < L; l++)
+        if (items[l]) atomicAdd(&d.ctr->levelCount[l], items[l]);
     }
   }
   if (kWrite && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -642,36 +640,32 @@ __global__ void k_excl(Dev d) {
   }
 }
 
-// 13. Work items (iBlock | tiles << 22, first candidate).  The head segment
-//     holds every block's leading candidates in items of d.tilesPerWork
-//     tiles, the tail segment after it every block's last d.tailTiles
-//     candidates in items of d.tailTileSize.  The pair kernel's warps take
+// 13. Work items (iBlock | tiles << 22, first candidate), by level: all
+//     level-0 items (tilesPerWork tiles) first, then the level-1 items, and
+//     so on down to 1-tile items (work_split).  The pair kernel's warps take
 //     items in list order, so the last items they take are small and the
-//     warps finish close together.
+//     warps finish close together.  Within a level the order follows the
+//     atomics; the items themselves depend on their block only.
 __global__ void k_work(Dev d) {
   const int B = d.ctr->blockCount;
-  const int head = d.workOffset[d.maxBlocks];
+  int off[kWorkLevels + 1];
+  off[0] = 0;
+  for (int l = 0; l < kWorkLevels; l++) off[l + 1] = off[l] + d.ctr->levelCount[l];
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t == 0) {
-    int total = head + d.workTailOffset[d.maxBlocks];
+    const int total = off[kWorkLevels];
     d.ctr->workCount = total < d.capWork ? total : d.capWork;
     if (total > d.capWork) atomicOr(&d.ctr->status, kStatusWorkOverflow);
   }
   for (int b = t; b < B; b += gridDim.x * blockDim.x) {
-    const int c0 = d.candStart[b], c1 = d.candStart[b + 1];
-    const int nw = d.workCountPerBlock[b], nt = d.workTailCount[b];
-    const int mid = c1 - (c1 - c0 < d.tailTiles ? c1 - c0 : d.tailTiles);  // first tail candidate
-    int w0 = d.workOffset[b], s = c0;
-    for (int k = 0; k < nw; k++, s += d.tilesPerWork) {
-      const int n = mid - s < d.tilesPerWork ? mid - s : d.tilesPerWork;
-      if (w0 + k < d.capWork) d.work[w0 + k] = make_int2(b | (n << 22), s);
-    }
-    s = mid;
-    w0 = head + d.workTailOffset[b];
-    for (int k = 0; k < nt; k++, s += d.tailTileSize) {
-      const int n = c1 - s < d.tailTileSize ? c1 - s : d.tailTileSize;
-      if (w0 + k < d.capWork) d.work[w0 + k] = make_int2(b | (n << 22), s);
-    }
+    const int c0 = d.candStart[b], nc = d.candStart[b + 1] - c0;
+    int tiles[kWorkLevels], items[kWorkLevels];
+    work_split(nc, d.tilesPerWork, d.tailTiles, tiles, items);
+    int base = 0;
+    work_walk(c0, nc, d.tilesPerWork, d.tailTiles, [&](int l, int k, int first, int n) {
+      if (k == 0) base = off[l] + atomicAdd(&d.ctr->levelFill[l], items[l]);
+      if (base + k < d.capWork) d.work[base + k] = make_int2(b | (n << 22), first);
+    });
   }
 }
 
@@ -721,10 +715,6 @@ int rebuild_list(const Dev &d, const int *colRep, const float *pos, float rcull2
   launches += scan_exclusive(d.candFlag, d.candMaskOff, d.capCand, d.candMaskOff + d.capCand, d.scanPartial, s);
   k_excl<true><<<exGrid, 256, 0, s>>>(d);  // also maskCount
   // work items
-  launches += scan_exclusive(d.workCountPerBlock, d.workOffset, d.maxBlocks, d.workOffset + d.maxBlocks,
-                 d.scanPartial, s);
-  launches += scan_exclusive(d.workTailCount, d.workTailOffset, d.maxBlocks, d.workTailOffset + d.maxBlocks,
-                 d.scanPartial, s);
   k_work<<<grid_for(d.maxBlocks, 256), 256, 0, s>>>(d);
   return launches;
 }
