@@ -5,7 +5,10 @@ libbnb binding of oracle/dropin/bnb_dropin.cu (oracle/dropin/Makefile), runs
 through its own parser, structure and parameter code and Potential::initialize
 -- and both print their energy terms (display_nrg, src/io/io.cxx:386-395).
 The direct-space term eenbdirect must agree; every other term comes from the
-same reference code in both builds and must be identical."""
+same reference code in both builds and must agree to the resolution of the
+printed value: the reference sums its PME charge grid and its energies with
+floating-point atomics, so even two runs of the unmodified program can differ
+in the last printed digit."""
 import os
 import subprocess
 
@@ -21,6 +24,8 @@ TERMS = ["bond", "angle", "urey", "dihe", "impr", "cmap", "nb14", "nbdirect", "n
 NBDIRECT = TERMS.index("nbdirect")
 SUMS = {TERMS.index(t) for t in ("potential", "total", "nbdirect")}
 ENERGY_TOL = 1e-5                                 # eenbdirect difference per max(|E|, atoms)
+PRINT_TOL = 1e-4                                  # one unit of the last printed digit (display_nrg, %.4f)
+ATOMIC_TOL = 2e-7                                 # relative: FP32 atomic summation order in the reference
 CASES = {"water216": ("energy_water216.inp", 648), "dhfr": ("energy_dhfr.inp", 23558)}
 
 
@@ -54,4 +59,4 @@ def test_patched_reference_matches_unpatched(cuda, case, tmp_path):
         (e_bnb[NBDIRECT], e_ref[NBDIRECT])
     for k in range(len(TERMS)):
         if k not in SUMS:
-            assert e_bnb[k] == e_ref[k], (TERMS[k], e_bnb[k], e_ref[k])
+            assert abs(e_bnb[k] - e_ref[k]) <= PRINT_TOL + ATOMIC_TOL * abs(e_ref[k]), (TERMS[k], e_bnb[k], e_ref[k])
