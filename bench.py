@@ -146,9 +146,12 @@ class ClockSampler:
                 "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
-def ncu_profile_value(key):
-    """A figure of the committed ncu summary of the pair kernel (``key: value``), if any."""
-    path = os.path.join(ROOT, "profiles", "pair_kernel_chain_water_23558.md")
+PROFILES = {"chain_water_23558": "pair_kernel_chain_water_23558.md", "dhfr": "pair_kernel_dhfr_23558.md"}
+
+
+def ncu_profile_value(key, workload="chain_water_23558"):
+    """A figure of the committed ncu summary of the workload's pair kernel (``key: value``), if any."""
+    path = os.path.join(ROOT, "profiles", PROFILES[workload])
     try:
         for line in open(path):
             if line.strip().startswith(key + ":"):
@@ -158,9 +161,9 @@ def ncu_profile_value(key):
     return None
 
 
-def ncu_traffic_per_launch():
+def ncu_traffic_per_launch(workload="chain_water_23558"):
     """DRAM bytes per pair-kernel launch from the committed ncu summary, if any."""
-    return ncu_profile_value("traffic_bytes_per_launch")
+    return ncu_profile_value("traffic_bytes_per_launch", workload)
 
 
 # ---------------------------------------------------------------------------
@@ -440,7 +443,7 @@ def run_bnb(args, rank, world):
     pair_s = prof["pair_ms"] / 1e3
     achieved = P * FLOPS_PER_PAIR / pair_s / 1e12
     peak_t = peak.value / 1e12
-    traffic = ncu_traffic_per_launch()
+    traffic = ncu_traffic_per_launch(args.workload)
     line = {
         "metric": "nbdirect pairs/s", "value": value, "unit": "pairs/s", "n_gpus": world, "steps": K,
         "warmup": W, "ms_per_step": 1e3 * t_total / K, "higher_is_better": True, "scaling": "weak",
@@ -453,7 +456,7 @@ def run_bnb(args, rank, world):
                      "frac": achieved / peak_t, "traffic": traffic,
                      "kernel": "k_pair<PME,VFSWITCH> (per-launch mean over a second pass of the timed steps, CUDA events on its stream)",
                      "flops_per_pair": FLOPS_PER_PAIR, "peak_source": "measured FP32 FMA chains (bnb_fp32_peak)",
-                     "mufu_pipe_pct_ncu": ncu_profile_value("mufu_pipe_pct"),
+                     "mufu_pipe_pct_ncu": ncu_profile_value("mufu_pipe_pct", args.workload),
                      "pair_kernel_ms_mean": prof["pair_ms"] / max(1, prof["pair_launches"])},
         "rebuild_ms_mean": prof["rebuild_ms"] / max(1, prof["rebuilds"]),
         "ns_per_day_nbdirect_only": (K / t_total) * DT_FS * 86400 / 1e6,
