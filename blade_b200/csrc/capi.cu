@@ -401,7 +401,6 @@ const char *bnb_version(void) { return "bnb 0.1 (sm_100a)"; }
 
 int bnb_set_box_type(bnb_handle *h, int triclinic) {
   if (!h || (triclinic != 0 && triclinic != 1)) return BNB_ERR_ARG;
-  if (triclinic && h->pmeOrder) return BNB_ERR_UNSUPPORTED;  // PME grids are orthorhombic here
   if (h->triclinic != triclinic) {
     h->triclinic = triclinic;
     h->listBuilt = false;  // the next rebuild reads the boxes in the new layout
@@ -1235,24 +1234,30 @@ bnb::PmeArgs pme_args(bnb_handle *h, const float *position, const float *lambda)
   a.accL = h->pmeAccL;
   a.accE = h->pmeAccE;
   a.done = h->pmeDone;
+  a.tric = h->triclinic;
   return a;
 }
 }  // namespace
 
 extern "C" int bnb_set_pme(bnb_handle *h, int order, float gridSpace, const int *grid, const float *boxes) {
-  if (h && h->triclinic) return BNB_ERR_UNSUPPORTED;  // PME grids are orthorhombic here
   if (!h || !boxes || (order != 4 && order != 6 && order != 8) || (!grid && !(gridSpace > 0.f)))
     return BNB_ERR_ARG;
   if (!h->topo) return BNB_ERR_STATE;
   const int R = h->R;
   std::vector<bnb::PmeRep> pr(R);
-  for (int r = 0; r < R; r++)
+  for (int r = 0; r < R; r++) {
+    // grid sizes from the edge lengths |A|, |B|, |C| (potential.cxx:1206, box.a)
+    float b[3], t[3];
+    box_of(h, boxes, r, b, t);
+    const double len[3] = {(double)b[0], std::sqrt((double)t[0] * t[0] + (double)b[1] * b[1]),
+                           std::sqrt((double)t[1] * t[1] + (double)t[2] * t[2] + (double)b[2] * b[2])};
     for (int k = 0; k < 3; k++) {
-      if (!(boxes[3 * r + k] > 0.f)) return BNB_ERR_ARG;
-      const int K = grid ? grid[3 * r + k] : pme_grid_size(boxes[3 * r + k], gridSpace);
+      if (!(b[k] > 0.f) || !std::isfinite(len[k])) return BNB_ERR_ARG;
+      const int K = grid ? grid[3 * r + k] : pme_grid_size((float)len[k], gridSpace);
       if (K < order || K > 4096) return BNB_ERR_ARG;
       pr[r].K[k] = K;
     }
+  }
   // Grids are laid out grouped by size (stable in replica order), so every
   // set of equal grids is one batched FFT plan.
   std::vector<int> layout(R);

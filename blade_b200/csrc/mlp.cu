@@ -9,7 +9,8 @@
 //   MSE loss         L = (1/M) sum_m sum_n w_n w_mn (Y - T)^2, dY = dL/dY
 //   Adam             FP32 master weights, BF16 working copy
 // Every product takes BF16 operands (round to nearest even) and accumulates
-// in FP32 in a fixed order, so results are reproducible run to run.  act is
+// in FP32 in a fixed order on the tensor pipe (mma.sync m16n8k16), so results
+// are reproducible run to run.  act is
 // 0 (identity) or 1 (SiLU, z * sigmoid(z)).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -19,55 +20,81 @@
 
 namespace {
 
-__device__ __forceinline__ float bf2f(uint16_t v) { return __uint_as_float((uint32_t)v << 16); }
 __device__ __forceinline__ uint16_t f2bf(float f) {
   __nv_bfloat16 h = __float2bfloat16_rn(f);
   return *reinterpret_cast<uint16_t *>(&h);
 }
 __device__ __forceinline__ float sigmoid(float z) { return 1.f / (1.f + expf(-z)); }
 
-// C[i,j] (+)= sum_l A(i,l) B(l,j) over BF16 operands given by strides:
+// C[i,j] = sum_l A(i,l) B(l,j) over BF16 operands given by strides:
 // A(i,l) = A[i*sai + l*sal], B(l,j) = B[l*sbl + j*sbj]; C row-major [I,J].
-// 64x64 output tile per 256-thread CTA, 4x4 per thread, K staged in 16s.
-constexpr int kT = 64, kK = 16;
+// On the tensor pipe: a 64x64 output tile per 256-thread CTA, K staged in
+// 64s through shared memory (A as [row][k], B as [column][k]), each of the
+// 8 warps (2 x 4) computing 32x16 of the tile as 2 x 2 mma.m16n8k16 with
+// BF16 operands and FP32 accumulators, k steps of 16 in increasing order.
+constexpr int kT = 64, kK = 64, kPad = 8;
+
+__device__ __forceinline__ void mma_bf16_16816(float (&c)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
 
 __global__ void __launch_bounds__(256) k_gemm_bf16(int I, int J, int Lk, const uint16_t *A, long long sai,
                                                    long long sal, const uint16_t *B, long long sbl,
                                                    long long sbj, float *C) {
-  __shared__ float sA[kK][kT + 1];
-  __shared__ float sB[kK][kT + 1];
+  __shared__ __align__(16) uint16_t sA[kT][kK + kPad];  // [tile row][k]
+  __shared__ __align__(16) uint16_t sB[kT][kK + kPad];  // [tile column][k]
   const int i0 = blockIdx.y * kT, j0 = blockIdx.x * kT;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  float acc[4][4] = {};
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wm = warp >> 2, wn = warp & 3;  // warp tile: rows wm*32.., columns wn*16..
+  const int g = lane >> 2, t = lane & 3;    // mma fragment coordinates
+  float acc[2][2][4] = {};
   for (int l0 = 0; l0 < Lk; l0 += kK) {
     for (int e = threadIdx.x; e < kK * kT; e += 256) {
-      const int r = e % kT, l = e / kT;  // r: row of the tile, l: k index
-      const int gi = i0 + r, gl = l0 + l, gj = j0 + r;
-      sA[l][r] = (gi < I && gl < Lk) ? bf2f(A[gi * sai + gl * sal]) : 0.f;
-      sB[l][r] = (gj < J && gl < Lk) ? bf2f(B[gl * sbl + gj * sbj]) : 0.f;
+      const int r = e / kK, l = e % kK;  // r: tile row (A) or column (B), l: k index
+      const int gi = i0 + r, gj = j0 + r, gl = l0 + l;
+      sA[r][l] = (gi < I && gl < Lk) ? A[gi * sai + gl * sal] : (uint16_t)0;
+      sB[r][l] = (gj < J && gl < Lk) ? B[gl * sbl + gj * sbj] : (uint16_t)0;
     }
     __syncthreads();
 #pragma unroll
-    for (int l = 0; l < kK; l++) {
-      float a[4], b[4];
+    for (int ks = 0; ks < kK; ks += 16) {
+      uint32_t af[2][4], bfr[2][2];
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        a[u] = sA[l][ty + 16 * u];
-        b[u] = sB[l][tx + 16 * u];
+      for (int mt = 0; mt < 2; mt++) {
+        const int rb = wm * 32 + mt * 16;
+        af[mt][0] = *reinterpret_cast<const uint32_t *>(&sA[rb + g][ks + 2 * t]);
+        af[mt][1] = *reinterpret_cast<const uint32_t *>(&sA[rb + g + 8][ks + 2 * t]);
+        af[mt][2] = *reinterpret_cast<const uint32_t *>(&sA[rb + g][ks + 2 * t + 8]);
+        af[mt][3] = *reinterpret_cast<const uint32_t *>(&sA[rb + g + 8][ks + 2 * t + 8]);
       }
 #pragma unroll
-      for (int u = 0; u < 4; u++)
+      for (int nt = 0; nt < 2; nt++) {
+        const int cb = wn * 16 + nt * 8;
+        bfr[nt][0] = *reinterpret_cast<const uint32_t *>(&sB[cb + g][ks + 2 * t]);
+        bfr[nt][1] = *reinterpret_cast<const uint32_t *>(&sB[cb + g][ks + 2 * t + 8]);
+      }
 #pragma unroll
-        for (int v = 0; v < 4; v++) acc[u][v] = fmaf(a[u], b[v], acc[u][v]);
+      for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++) mma_bf16_16816(acc[mt][nt], af[mt], bfr[nt]);
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int u = 0; u < 4; u++)
+  for (int mt = 0; mt < 2; mt++)
 #pragma unroll
-    for (int v = 0; v < 4; v++) {
-      const int gi = i0 + ty + 16 * u, gj = j0 + tx + 16 * v;
-      if (gi < I && gj < J) C[(size_t)gi * J + gj] = acc[u][v];
+    for (int nt = 0; nt < 2; nt++) {
+      const int row = i0 + wm * 32 + mt * 16 + g, col = j0 + wn * 16 + nt * 8 + 2 * t;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {  // h = 0: row g, h = 1: row g + 8
+        const int r = row + 8 * h;
+        if (r < I && col < J) C[(size_t)r * J + col] = acc[mt][nt][2 * h];
+        if (r < I && col + 1 < J) C[(size_t)r * J + col + 1] = acc[mt][nt][2 * h + 1];
+      }
     }
 }
 
@@ -95,13 +122,21 @@ __global__ void k_act_grad(int M, int N, const float *dY, const float *Z, int ac
   dZb[t] = f2bf(g);
 }
 
-// db[n] = sum_m dZ[m,n], rows added in order.
-__global__ void k_colsum(int M, int N, const float *dZ, float *db) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
+// db[n] = sum_m dZ[m,n]: 32 columns per 256-thread CTA, 8 row slices per
+// column (slice r sums rows r, r+8, ... in order), the slices then added in a
+// fixed tree order -- parallel and reproducible.
+__global__ void __launch_bounds__(256) k_colsum(int M, int N, const float *dZ, float *db) {
+  __shared__ float part[8][33];
+  const int c = threadIdx.x & 31, r = threadIdx.x >> 5;
+  const int n = blockIdx.x * 32 + c;
   float s = 0.f;
-  for (int m = 0; m < M; m++) s += dZ[(size_t)m * N + n];
-  db[n] = s;
+  if (n < N)
+    for (int m = r; m < M; m += 8) s += dZ[(size_t)m * N + n];
+  part[r][c] = s;
+  __syncthreads();
+  if (r == 0 && n < N)
+    db[n] = ((part[0][c] + part[1][c]) + (part[2][c] + part[3][c])) +
+            ((part[4][c] + part[5][c]) + (part[6][c] + part[7][c]));
 }
 
 // One CTA: loss and dY of the weighted mean squared error, summed in a fixed order.
@@ -177,7 +212,7 @@ extern "C" int bnb_mlp_linear_backward(int M, int N, int K, const float *dY, con
   if (M == 0 || N == 0) return BNB_OK;
   cudaStream_t s = (cudaStream_t)stream;
   k_act_grad<<<grid1((long long)M * N), 256, 0, s>>>(M, N, dY, Z, act, dZ, dZb);
-  k_colsum<<<grid1(N), 256, 0, s>>>(M, N, dZ, db);
+  k_colsum<<<(N + 31) / 32, 256, 0, s>>>(M, N, dZ, db);
   int rc = gemm(N, K, M, dZb, 1, N, X, K, 1, dW, s);  // dW[n,k] = sum_m dZ[m,n] X[m,k]
   if (rc) return rc;
   if (dX) {

@@ -18,6 +18,12 @@
 //   * lanes of an atom's 8-lane group own z offsets (contiguous grid
 //     addresses within one instruction) instead of x/y/z parity classes;
 //   * R replicas with their own grids in one launch per phase.
+// Triclinic cells (the reference's flagBox branch): the fractional
+// coordinates s = H^-1 x of the cell matrix H (columns A, B, C) replace x / L
+// (nbrecip.cu:116-178), here by back substitution in FP64; the wave vectors
+// are H^-T m (nbrecip.cu:236-242) and dU/dx = H^-T dU/ds (nbrecip.cu:456-462),
+// with H^-1 as the reference's State::kTricBox_f (state.cxx:485-491).
+// Orthorhombic handles keep the plain per-dimension path.
 // The 3-D FFTs are cuFFT plans (one batched plan per run of consecutive
 // replicas with equal grids), as in the reference.
 #include <cuda_runtime.h>
@@ -80,6 +86,51 @@ __device__ __forceinline__ void grid_coord(float x, int K, float L, int &i0, flo
   if (i0 < 0) i0 += K;
 }
 
+// Grid index (mod K) and fraction of a coordinate already in grid units.
+__device__ __forceinline__ void grid_index(double u, int K, int &i0, float &frac) {
+  const double u0 = floor(u);
+  frac = (float)(u - u0);
+  double m = u0 - (double)K * floor(u0 / (double)K);
+  i0 = (int)m;
+  if (i0 >= K) i0 -= K;
+  if (i0 < 0) i0 += K;
+}
+
+// Grid coordinates of an atom in its replica's cell (both box types).
+__device__ __forceinline__ void grid_coords(const PmeArgs &a, const float *x, const PmeRep &pr, const RepInfo &ri,
+                                            int (&i0)[3], float (&f)[3]) {
+  if (!a.tric) {
+    for (int d = 0; d < 3; d++) grid_coord(x[d], pr.K[d], ri.box[d], i0[d], f[d]);
+    return;
+  }
+  // box = (A_x, B_y, C_z), tric = (B_x, C_x, C_y)
+  const double sz = (double)x[2] / (double)ri.box[2];
+  const double sy = ((double)x[1] - (double)ri.tric[2] * sz) / (double)ri.box[1];
+  const double sx = ((double)x[0] - (double)ri.tric[0] * sy - (double)ri.tric[1] * sz) / (double)ri.box[0];
+  grid_index(sx * pr.K[0], pr.K[0], i0[0], f[0]);
+  grid_index(sy * pr.K[1], pr.K[1], i0[1], f[1]);
+  grid_index(sz * pr.K[2], pr.K[2], i0[2], f[2]);
+}
+
+// H^-1 of a triclinic cell as (xx, xy, xz, yy, yz, zz), FP32 like the
+// reference's kTricBox_f.
+struct RecipCell {
+  float xx, xy, xz, yy, yz, zz;
+};
+__device__ __forceinline__ RecipCell recip_cell(const RepInfo &ri) {
+  const float ax = ri.box[0], by = ri.box[1], cz = ri.box[2];
+  const float bx = ri.tric[0], cx = ri.tric[1], cy = ri.tric[2];
+  const float vinv = 1.f / (ax * by * cz);
+  RecipCell k;
+  k.xx = by * cz * vinv;
+  k.xy = -bx * cz * vinv;
+  k.xz = (bx * cy - by * cx) * vinv;
+  k.yy = cz * ax * vinv;
+  k.yz = -cy * ax * vinv;
+  k.zz = ax * by * vinv;
+  return k;
+}
+
 __device__ __forceinline__ float atom_scale(const PmeArgs &a, int atom, int &block) {
   block = a.siteBlock[atom] & 0xFFFF;
   return (block && a.lambda) ? a.lambda[block] : 1.f;
@@ -101,14 +152,13 @@ __global__ void __launch_bounds__(256) k_spread(PmeArgs a) {
   const float qe = a.q[atom] * atom_scale(a, atom, block);
   if (qe == 0.f) return;
   float wx[ORDER], wy[ORDER], wz[ORDER], d[ORDER];
-  int ix0, iy0, iz0;
-  float f;
-  grid_coord(a.x[3 * atom], pr.K[0], ri.box[0], ix0, f);
-  bspline<ORDER>(f, wx, d);
-  grid_coord(a.x[3 * atom + 1], pr.K[1], ri.box[1], iy0, f);
-  bspline<ORDER>(f, wy, d);
-  grid_coord(a.x[3 * atom + 2], pr.K[2], ri.box[2], iz0, f);
-  bspline<ORDER>(f, wz, d);
+  int i0[3];
+  float f[3];
+  grid_coords(a, a.x + 3 * atom, pr, ri, i0, f);
+  const int ix0 = i0[0], iy0 = i0[1], iz0 = i0[2];
+  bspline<ORDER>(f[0], wx, d);
+  bspline<ORDER>(f[1], wy, d);
+  bspline<ORDER>(f[2], wz, d);
   float wzg = wz[0];
 #pragma unroll
   for (int k = 1; k < ORDER; k++) wzg = g == k ? wz[k] : wzg;
@@ -151,6 +201,7 @@ __global__ void k_convolve(PmeArgs a) {
   const int K0 = pr.K[0], K1 = pr.K[1], K2h = pr.K[2] / 2 + 1;
   const int n = K0 * K1 * K2h;
   const float ix = 1.f / ri.box[0], iy = 1.f / ri.box[1], iz = 1.f / ri.box[2];
+  const RecipCell rc = a.tric ? recip_cell(ri) : RecipCell{};
   const float c = (float)(1.0 / (2.0 * kPi * (double)ri.box[0] * (double)ri.box[1] * (double)ri.box[2]));
   const float g = (float)(kPi * kPi / ((double)a.beta * (double)a.beta));
   const float *m0 = a.mod + pr.modOff, *m1 = m0 + K0, *m2 = m1 + K1;
@@ -160,9 +211,17 @@ __global__ void k_convolve(PmeArgs a) {
     const int row = e / K2h;
     const int j = row % K1;
     const int i = row / K1;
-    const float kx = (float)(2 * i <= K0 ? i : i - K0) * ix;
-    const float ky = (float)(2 * j <= K1 ? j : j - K1) * iy;
-    const float kz = (float)k * iz;
+    const float mi = (float)(2 * i <= K0 ? i : i - K0), mj = (float)(2 * j <= K1 ? j : j - K1), mk = (float)k;
+    float kx, ky, kz;
+    if (!a.tric) {
+      kx = mi * ix;
+      ky = mj * iy;
+      kz = mk * iz;
+    } else {  // k = H^-T m
+      kx = mi * rc.xx;
+      ky = fmaf(mi, rc.xy, mj * rc.yy);
+      kz = fmaf(mi, rc.xz, fmaf(mj, rc.yz, mk * rc.zz));
+    }
     const float k2 = fmaf(kx, kx, fmaf(ky, ky, kz * kz));
     const float factor = e == 0 ? 0.f : m0[i] * m1[j] * m2[k] * c * expf(-g * k2) / k2;
     float2 v = spec[e];
@@ -228,14 +287,13 @@ __global__ void __launch_bounds__(256) k_gather(PmeArgs a, bnb_outputs o) {
     qe = qraw * atom_scale(a, atom, block);
     if (g < ORDER) {
       float wx[ORDER], wy[ORDER], wz[ORDER], dx[ORDER], dy[ORDER], dz[ORDER];
-      int ix0, iy0, iz0;
-      float f;
-      grid_coord(a.x[3 * atom], pr.K[0], ri.box[0], ix0, f);
-      bspline<ORDER>(f, wx, dx);
-      grid_coord(a.x[3 * atom + 1], pr.K[1], ri.box[1], iy0, f);
-      bspline<ORDER>(f, wy, dy);
-      grid_coord(a.x[3 * atom + 2], pr.K[2], ri.box[2], iz0, f);
-      bspline<ORDER>(f, wz, dz);
+      int i0[3];
+      float f[3];
+      grid_coords(a, a.x + 3 * atom, pr, ri, i0, f);
+      const int ix0 = i0[0], iy0 = i0[1], iz0 = i0[2];
+      bspline<ORDER>(f[0], wx, dx);
+      bspline<ORDER>(f[1], wy, dy);
+      bspline<ORDER>(f[2], wz, dz);
       float wzg = wz[0], dzg = dz[0];
 #pragma unroll
       for (int k = 1; k < ORDER; k++) {
@@ -279,9 +337,18 @@ __global__ void __launch_bounds__(256) k_gather(PmeArgs a, bnb_outputs o) {
   if (valid && g == 0) {
     const RepInfo &ri = a.rep[r];
     const float c = 2.f * qe;
-    const float fx = c * gx * ((float)pr.K[0] / ri.box[0]);
-    const float fy = c * gy * ((float)pr.K[1] / ri.box[1]);
-    const float fz = c * gz * ((float)pr.K[2] / ri.box[2]);
+    float fx, fy, fz;
+    if (!a.tric) {
+      fx = c * gx * ((float)pr.K[0] / ri.box[0]);
+      fy = c * gy * ((float)pr.K[1] / ri.box[1]);
+      fz = c * gz * ((float)pr.K[2] / ri.box[2]);
+    } else {  // dU/dx = H^-T dU/ds
+      const RecipCell k = recip_cell(ri);
+      const float hx = c * gx * (float)pr.K[0], hy = c * gy * (float)pr.K[1], hz = c * gz * (float)pr.K[2];
+      fx = hx * k.xx;
+      fy = fmaf(hx, k.xy, hy * k.yy);
+      fz = fmaf(hx, k.xz, fmaf(hy, k.yz, hz * k.zz));
+    }
     if (o.force64) {
       out64(&o.force64[3 * atom], fx, a.mode);
       out64(&o.force64[3 * atom + 1], fy, a.mode);

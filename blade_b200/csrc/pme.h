@@ -34,6 +34,7 @@ struct PmeArgs {
   long long *accE;         // [R]
   unsigned int *done;      // CTAs finished in the current gather / self launch (zero between launches)
   int mode;                // BNB_OUT_SET / BNB_OUT_ADD64 bits of the call
+  int tric;                // boxes are triclinic cells (RepInfo::box and ::tric)
 };
 
 // Spread lambda-scaled charges into qfix and convert to the FP32 grid

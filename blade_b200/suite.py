@@ -31,8 +31,9 @@ def _gen_replica(args):
     return systems.msld_chain(seed, n, sites, subs)
 
 
-def batch_replicas(n_rep=64, seed=4, workers=None):
-    """systems.batch_replicas, generated in parallel (spawned workers, no CUDA in them)."""
+def replica_specs(n_rep=64, seed=4):
+    """(seed, atoms, sites, substituents per site) of the batched replicas:
+    atom counts log-uniform in 3k-30k, 1-3 sites of 2-5 substituents."""
     rng = np.random.default_rng(seed)
     specs = []
     for r in range(n_rep):
@@ -40,9 +41,98 @@ def batch_replicas(n_rep=64, seed=4, workers=None):
         ns = int(rng.integers(1, 4))
         subs = [int(k) for k in rng.integers(2, 6, ns)]
         specs.append((seed * 1000 + r, n, ns, subs))
+    return specs
+
+
+def batch_replicas(n_rep=64, seed=4, workers=None, only=None):
+    """systems.batch_replicas, generated in parallel (spawned workers, no CUDA
+    in them); ``only``: the indices to generate (default all)."""
+    specs = replica_specs(n_rep, seed)
+    if only is not None:
+        specs = [specs[i] for i in only]
     workers = workers or min(16, os.cpu_count() or 1)
     with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
         return list(ex.map(_gen_replica, specs))
+
+
+def replica_weights(specs, r_cut=12.0):
+    """Load of each replica for the partition over ranks: its estimated pairs."""
+    from .replicas import pair_estimate
+    return [pair_estimate(n, n / systems.MSLD_CHAIN_DENSITY, r_cut) for _, n, _, _ in specs]
+
+
+def run_batch_ranks(args):
+    """The batched run over the ranks of torchrun (one GPU each): whole
+    replicas per rank, balanced by estimated pairs (blade_b200.replicas), each
+    rank stepping its own on one handle under a CUDA graph; no collective in
+    the step loop.  Rank 0 prints the slowest rank's device time and the
+    aggregate ns/day of all replicas."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from .batch import MsldBatch, ns_per_day
+    from .replicas import gather_rows, imbalance, partition
+    rank, world = int(os.environ["RANK"]), int(os.environ["WORLD_SIZE"])
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    try:
+        specs = replica_specs(args.replicas, args.seed)
+        weights = replica_weights(specs)
+        parts = partition(weights, world)
+        mine = parts[rank]
+        reps = batch_replicas(args.replicas, seed=args.seed, only=mine,
+                              workers=max(1, min(16, os.cpu_count() or 1) // world)) if mine else []
+        K = args.steps
+        t_rank, st, nan, tuning = 0.0, 0, 0, None
+        B = None
+        if reps:
+            B = MsldBatch(reps, tune=True, constraints=args.constraints, pme=args.pme)
+            tuning = B.tuning()
+            B.capture()
+            B.run_graph(20)
+        torch.cuda.synchronize()
+        dist.barrier()
+        if B is not None:
+            a, b = _events()
+            a.record()
+            B.run_graph(K)
+            b.record()
+            torch.cuda.synchronize()
+            t_rank = a.elapsed_time(b) / 1e3
+            st, nan = B.check()
+        dist.barrier()
+        t = torch.tensor([t_rank, float(st != 0), float(nan)], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        # per-replica statistics in global order: atoms and the final lambda sums
+        rows = torch.zeros((len(mine), 2), dtype=torch.float64, device=dev)
+        if B is not None:
+            for k, r in enumerate(reps):
+                rows[k, 0] = r.N
+            lam = B.lam.double()
+            starts = B.nb.lam_starts
+            for k in range(len(reps)):
+                rows[k, 1] = lam[starts[k]:starts[k + 1]].sum()
+        allrows = gather_rows(rows, mine, len(specs))
+        times = [torch.zeros(1, dtype=torch.float64, device=dev) for _ in range(world)]
+        dist.all_gather(times, torch.tensor([t_rank], dtype=torch.float64, device=dev))
+        if B is not None:
+            B.close()
+        if rank == 0:
+            R = len(specs)
+            line = {"config": f"{R} MSLD replicas over {world} ranks (whole replicas per rank, balanced by "
+                              "estimated pairs), rCut 12, PME+VFSWITCH, soft core, dt 2 fs",
+                    "replicas": R, "world": world, "steps": K, "scaling": "strong",
+                    "replicas_per_rank": [len(p) for p in parts],
+                    "estimated_load_imbalance": imbalance(weights, parts),
+                    "seconds_max_over_ranks": float(t[0]), "seconds_per_rank": [float(x.item()) for x in times],
+                    "ns_per_day_aggregate": ns_per_day(K, float(t[0]), replicas=R),
+                    "atoms_total": int(allrows[:, 0].sum().item()),
+                    "lambda_sum_per_site_ok": bool(torch.isfinite(allrows[:, 1]).all().item()),
+                    "status_bad": bool(t[1] > 0), "nan": float(t[2]), "tuning_rank0": tuning}
+            print(json.dumps(line), flush=True)
+    finally:
+        dist.destroy_process_group()
 
 
 def _events():
@@ -51,6 +141,8 @@ def _events():
 
 
 def run_batch(args):
+    if "RANK" in os.environ and "WORLD_SIZE" in os.environ:  # launched by torchrun
+        return run_batch_ranks(args)
     import torch
     from .batch import MsldBatch, ns_per_day
     t0 = time.time()

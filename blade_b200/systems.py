@@ -584,11 +584,14 @@ def msld_water(seed: int = 3, sites: int = 3, subs: int = 4, clear: float = 2.2,
                   bond_param=with_bond_lengths(xyz, bonds, kb))
 
 
+MSLD_CHAIN_DENSITY = 0.0965   # atoms per A^3 of the msld_chain replicas
+
+
 def msld_chain(seed: int, n_atoms: int, n_sites: int, subs_per_site, rCut=12.0, rSwitch=10.0,
                beta=0.32) -> System:
     """MSLD replica: chain solute + water + MSLD sites on chain atoms, density 0.0965 A^-3."""
     rng = np.random.default_rng(seed)
-    box = (n_atoms / 0.0965) ** (1 / 3)
+    box = (n_atoms / MSLD_CHAIN_DENSITY) ** (1 / 3)
     n_chain = max(60, int(0.1 * n_atoms))
     center = np.full(3, box / 2)
     radius = (3 * n_chain / (4 * math.pi * 0.06)) ** (1 / 3)

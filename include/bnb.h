@@ -109,9 +109,9 @@ int bnb_set_topology(bnb_handle *h, const bnb_nbond *nbonds,
  * reference's triclinic modulus does (src/main/real3.h:340-360), and the
  * half-shell images are centred under the shear as its cull does
  * (src/domdec/cull.cu:141-190); A_x, B_y and C_z must each be at least
- * 2 rCut.  Direct space, nb14/nbex and the list are supported; PME is not
- * (BNB_ERR_UNSUPPORTED from bnb_set_pme / bnb_compute_pme, and from this call
- * once PME is set).  Changing the type requires a synchronous rebuild.
+ * 2 rCut.  Direct space, nb14/nbex, the list and PME reciprocal space (the
+ * reference's flagBox branch of getforce_ewald) all take the cell.  Changing
+ * the type requires a synchronous rebuild.
  */
 int bnb_set_box_type(bnb_handle *h, int triclinic);
 
@@ -260,13 +260,17 @@ int bnb_compute_nbex(bnb_handle *h, const float *position, const float *lambda,
  *   gridSpace, grid  host int [3*replicas] grid sizes, or NULL for the
  *            reference's rule from the spacing (Run::gridSpace, default 1 A):
  *            per edge the smallest of j*{32,27,24,20,18} above L/gridSpace
- *   boxes    host float [3*replicas] edges the grids are sized for
+ *   boxes    host float [3*replicas] edges the grids are sized for, or
+ *            [6*replicas] triclinic cells (bnb_set_box_type): the grids are
+ *            sized for the edge lengths |A|, |B|, |C| (the reference's box.a)
  * Charges, MSLD blocks and replicas come from bnb_set_topology; an atom of
  * block b > 0 carries lambda_b q (Msld atomBlock, nbrecip.cu:101-106).
  * bnb_compute_pme evaluates the reciprocal term (spread, R2C, influence
  * function, C2R, gather) on position (device float [3N], State::position_fd)
- * and lambda (device float, State::lambda_fd) with the box edges `boxes`
- * (host float [3*replicas]; the grids stay as set), into `out` with
+ * and lambda (device float, State::lambda_fd) with the boxes `boxes` (host
+ * float [3*replicas] edges or [6*replicas] cells; the grids stay as set; in
+ * a triclinic cell the grid axes follow the fractional coordinates H^-1 x of
+ * the cell matrix H, nbrecip.cu:116-178, 236-242, 456-462), into `out` with
  * bnb_compute's output semantics; energies are the eenbrecip term.
  * bnb_compute_ewald_self adds the self term (energy eenbrecipself and
  * dU/dlambda; no spatial force).  Both do nothing unless elecMethod is PME

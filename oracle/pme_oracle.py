@@ -26,6 +26,15 @@ src/msld/msld.cu:470-476).
 
 ``ewald_recip_exact`` is the plain Ewald reciprocal sum over k vectors, an
 independent check that the restatement converges to the right physics.
+
+Triclinic cells (the flagBox branch of the same kernels; the box given as the
+6 floats (A_x, B_y, C_z, B_x, C_x, C_y) of a lower-triangular cell A = (A_x,
+0, 0), B = (B_x, B_y, 0), C = (C_x, C_y, C_z)): the fractional coordinates
+s = H^-1 x (H the cell matrix with columns A, B, C; State::kTricBox_f,
+src/system/state.cxx:485-491, holds H^-1) replace x / L, so u_d = K_d s_d
+(nbrecip.cu:116-178); the wave vectors are k = H^-T m (nbrecip.cu:236-242);
+dU/dx = H^-T (dU/ds) (nbrecip.cu:456-462); V = A_x B_y C_z; the grid sizes
+come from the edge lengths |A|, |B|, |C| (potential.cxx:1206, box.a).
 """
 from __future__ import annotations
 
@@ -102,11 +111,41 @@ def atom_lambda(site_block, lam):
     return l, b
 
 
+def cell(box):
+    """(H, H^-1) of a box: 3 edge lengths or the 6-float triclinic cell."""
+    b = np.asarray(box, np.float64).reshape(-1)
+    if len(b) == 3:
+        H = np.diag(b)
+    else:
+        H = np.array([[b[0], b[3], b[4]], [0.0, b[1], b[5]], [0.0, 0.0, b[2]]])
+    return H, np.linalg.inv(H)
+
+
+def edge_lengths(box):
+    """|A|, |B|, |C| of a box (3 or 6 floats): the lengths the grid sizes use."""
+    H, _ = cell(box)
+    return np.sqrt((H * H).sum(0))
+
+
+def fractional(xyz, box):
+    """s = H^-1 x by back substitution (z first), FP64."""
+    b = np.asarray(box, np.float64).reshape(-1)
+    x = np.asarray(xyz, np.float64)
+    if len(b) == 3:
+        return x / b
+    sz = x[:, 2] / b[2]
+    sy = (x[:, 1] - b[5] * sz) / b[1]
+    sx = (x[:, 0] - b[3] * sy - b[4] * sz) / b[0]
+    return np.stack([sx, sy, sz], 1)
+
+
 def pme_recip(xyz, q, box, K, order, beta, kElectric, site_block=None, lam=None):
-    """(energy, dU/dx [N,3], dU/dlambda [L] or None, phi [N]) of one system."""
+    """(energy, dU/dx [N,3], dU/dlambda [L] or None, phi [N]) of one system;
+    box: 3 edge lengths or the 6-float triclinic cell."""
     xyz = np.asarray(xyz, np.float64)
     q = np.asarray(q, np.float64)
-    box = np.asarray(box, np.float64)
+    H, Hinv = cell(box)
+    frac = fractional(xyz, box)
     N = len(q)
     K = [int(k) for k in K]
     if site_block is None:
@@ -115,7 +154,7 @@ def pme_recip(xyz, q, box, K, order, beta, kElectric, site_block=None, lam=None)
     qe = l * q
     W, D, idx = [], [], []
     for d in range(3):
-        u = xyz[:, d] * K[d] / box[d]
+        u = frac[:, d] * K[d]
         u0 = np.floor(u)
         w, dw = weights(u - u0, order)
         W.append(w)
@@ -132,23 +171,26 @@ def pme_recip(xyz, q, box, K, order, beta, kElectric, site_block=None, lam=None)
     m1 = np.arange(K[0]); m1 = np.where(2 * m1 <= K[0], m1, m1 - K[0])
     m2 = np.arange(K[1]); m2 = np.where(2 * m2 <= K[1], m2, m2 - K[1])
     m3 = np.arange(K[2] // 2 + 1)
-    k2 = ((m1 / box[0])[:, None, None] ** 2 + (m2 / box[1])[None, :, None] ** 2
-          + (m3 / box[2])[None, None, :] ** 2)
+    # k = H^-T m
+    mm = np.stack(np.meshgrid(m1, m2, m3, indexing="ij"), -1).astype(np.float64)
+    kv = mm @ Hinv
+    k2 = (kv * kv).sum(-1)
     B = (moduli(K[0], order)[:, None, None] * moduli(K[1], order)[None, :, None]
          * moduli(K[2], order)[: K[2] // 2 + 1][None, None, :])
-    V = box[0] * box[1] * box[2]
+    V = H[0, 0] * H[1, 1] * H[2, 2]
     with np.errstate(divide="ignore", invalid="ignore"):
         G = B * (0.5 * kElectric / (np.pi * V)) * np.exp(-np.pi ** 2 * k2 / beta ** 2) / k2
     G[0, 0, 0] = 0.0
     phi_grid = np.fft.irfftn(F * G, s=K, axes=(0, 1, 2)) * (K[0] * K[1] * K[2])   # cuFFT C2R is unnormalised
     P = phi_grid[np.broadcast_to(ix, w3.shape), np.broadcast_to(iy, w3.shape), np.broadcast_to(iz, w3.shape)]
     phi = (P * w3).sum((1, 2, 3))
-    grad = np.zeros((N, 3))
+    gs = np.zeros((N, 3))          # dU/ds
     for d in range(3):
         parts = [W[0], W[1], W[2]]
         parts[d] = D[d]
         g3 = parts[0][:, :, None, None] * parts[1][:, None, :, None] * parts[2][:, None, None, :]
-        grad[:, d] = 2 * qe * (K[d] / box[d]) * (P * g3).sum((1, 2, 3))
+        gs[:, d] = 2 * qe * K[d] * (P * g3).sum((1, 2, 3))
+    grad = gs @ Hinv               # dU/dx = H^-T dU/ds
     energy = float((qe * phi).sum())
     lforce = None
     if lam is not None:
@@ -174,15 +216,16 @@ def ewald_self(q, beta, kElectric, site_block=None, lam=None):
 
 
 def ewald_recip_exact(xyz, q, box, beta, kElectric, kmax: int):
-    """Plain Ewald reciprocal energy and dU/dx over |m_d| <= kmax."""
+    """Plain Ewald reciprocal energy and dU/dx over |m_d| <= kmax (box: 3
+    edge lengths or the 6-float triclinic cell; k = H^-T m)."""
     xyz = np.asarray(xyz, np.float64)
     q = np.asarray(q, np.float64)
-    box = np.asarray(box, np.float64)
-    V = box.prod()
+    H, Hinv = cell(box)
+    V = H[0, 0] * H[1, 1] * H[2, 2]
     r = np.arange(-kmax, kmax + 1)
     m = np.stack(np.meshgrid(r, r, r, indexing="ij"), -1).reshape(-1, 3)
     m = m[np.any(m != 0, 1)]
-    k = m / box
+    k = m @ Hinv
     k2 = (k * k).sum(1)
     pref = kElectric / (2 * np.pi * V) * np.exp(-np.pi ** 2 * k2 / beta ** 2) / k2
     ph = 2 * np.pi * xyz @ k.T                      # [N, M]

@@ -701,5 +701,14 @@ extern "C" int ref_set_tric(ref_handle *h, const double *tric) {
   st->tricBox_f.c.x = (float)tric[3]; st->tricBox_f.c.y = (float)tric[4]; st->tricBox_f.c.z = (float)tric[5];
   st->orthBox.x = tric[0]; st->orthBox.y = tric[2]; st->orthBox.z = tric[5];
   st->orthBox_f.x = (float)tric[0]; st->orthBox_f.y = (float)tric[2]; st->orthBox_f.z = (float)tric[5];
+  // reciprocal cell the PME kernels read (State::kTricBox_f, as set by
+  // src/system/state.cxx:485-491 from tricBox_f, in the reference's real)
+  const real Vinv = 1 / (st->tricBox_f.a.x * st->tricBox_f.b.y * st->tricBox_f.c.z);
+  st->kTricBox_f.a.x = st->tricBox_f.b.y * st->tricBox_f.c.z * Vinv;
+  st->kTricBox_f.a.y = -st->tricBox_f.b.x * st->tricBox_f.c.z * Vinv;
+  st->kTricBox_f.a.z = (st->tricBox_f.b.x * st->tricBox_f.c.y - st->tricBox_f.b.y * st->tricBox_f.c.x) * Vinv;
+  st->kTricBox_f.b.x = st->tricBox_f.c.z * st->tricBox_f.a.x * Vinv;
+  st->kTricBox_f.b.y = -st->tricBox_f.c.y * st->tricBox_f.a.x * Vinv;
+  st->kTricBox_f.c.x = st->tricBox_f.a.x * st->tricBox_f.b.y * Vinv;
   return 0;
 }

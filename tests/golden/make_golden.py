@@ -29,7 +29,8 @@ and the reference's own CHARMM fixtures: `make_golden.py REFERENCE_ROOT
 fixture_<name>.npz, and `--real-only` (GPU) evaluates the reference's direct
 space, nb14, nbex, PME and self terms on them into real_<name>.npz; and the
 reference's triclinic direct space on triclinic water boxes, tric_*.npz
-(--tric-only).
+(--tric-only), and its triclinic PME reciprocal space on them,
+tric_pme_*.npz (--tric-pme-only).
 """
 import os
 import sys
@@ -242,11 +243,35 @@ def tric_cases(out):
         print("tric", name, s.N, r["energy"], flush=True)
 
 
+def tric_pme_cases(out):
+    """The reference's triclinic PME reciprocal space (the flagBox branch of
+    getforce_ewald with State::kTricBox_f) on the same two cells, order 6,
+    grids from the 1 A rule on the edge lengths."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle import pme_oracle
+    from test_gpu_triclinic import CASES
+    for name, make in CASES.items():
+        s = make()
+        K = [pme_oracle.grid_size(L, 1.0) for L in pme_oracle.edge_lengths(s.box6())]
+        ref = refgpu.RefGPU(s)
+        ref.set_pme(6, K)
+        r = ref.evaluate_pme("recip")
+        np.savez_compressed(os.path.join(out, f"tric_pme_{name}.npz"), case=np.str_(name),
+                            xyz=s.xyz.astype(np.float32), grad=r["grad"].astype(np.float32),
+                            energy=np.float64(r["energy"]), lambdaForce=r["lambdaForce"].astype(np.float64),
+                            K=np.int64(K), order=np.int64(6), tric_box=s.tric_box())
+        print("tric_pme", name, K, r["energy"], flush=True)
+
+
 def main(out, pairs_only=False, pme_only=False, holonomic_only=False, msld_only=False, real_only=False,
-         tric_only=False):
+         tric_only=False, tric_pme_only=False):
     os.makedirs(out, exist_ok=True)
+    if tric_pme_only:
+        tric_pme_cases(out)
+        return
     if tric_only:
         tric_cases(out)
+        tric_pme_cases(out)
         return
     if real_only:
         real_cases(out)
@@ -300,4 +325,4 @@ if __name__ == "__main__":
     main(args[0] if args else os.path.join(ROOT, "golden_out"), pairs_only="--pairs-only" in sys.argv,
          pme_only="--pme-only" in sys.argv, holonomic_only="--holonomic-only" in sys.argv,
          msld_only="--msld-only" in sys.argv, real_only="--real-only" in sys.argv,
-         tric_only="--tric-only" in sys.argv)
+         tric_only="--tric-only" in sys.argv, tric_pme_only="--tric-pme-only" in sys.argv)

@@ -114,3 +114,28 @@ def test_batch_with_complete_electrostatics(cuda):
     lam = B.lam.cpu().numpy()
     assert np.all(lam >= 0) and np.all(lam <= 1 + 1e-12)
     B.close()
+
+
+def test_suite_batch_over_ranks_under_torchrun(cuda):
+    """The rank path of `suite batch` (whole replicas per rank, balanced by
+    estimated pairs) under torchrun with one process: the partition, the
+    per-rank graph run, the max-over-ranks time and the gather of per-replica
+    rows all run through NCCL with world size 1."""
+    import json
+    import os
+    import socket
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=1", "--master-addr",
+           "127.0.0.1", "--master-port", str(port), "--module", "blade_b200.suite", "batch", "--replicas", "4",
+           "--steps", "20"]
+    r = subprocess.run(cmd, cwd=root, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-3000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["world"] == 1 and line["replicas"] == 4 and line["replicas_per_rank"] == [4]
+    assert not line["status_bad"] and line["nan"] == 0 and line["lambda_sum_per_site_ok"]
+    assert line["seconds_max_over_ranks"] > 0 and line["ns_per_day_aggregate"] > 0

@@ -3,7 +3,9 @@ path of getforce_nbdirect, Domdec's cull and wrap): the block list equals the
 CPU restatement bit for bit, forces and energies match the FP64 oracle (which
 sums every lattice image) and the reference's own triclinic CUDA path
 (tests/golden/tric_*.npz), the result does not change when atoms are moved by
-cell vectors, and PME, which is orthorhombic here, refuses the cell."""
+cell vectors; PME reciprocal space in the cell (the flagBox branch of
+getforce_ewald) matches the FP64 oracle, the reference's own triclinic PME
+(tests/golden/tric_pme_*.npz) and is unchanged by cell-vector moves."""
 import dataclasses
 import glob
 import os
@@ -100,15 +102,73 @@ def test_lattice_translations_change_nothing(cuda):
     nb.close()
 
 
-def test_pme_refuses_triclinic(cuda):
-    s = systems.water_box_tric()
+PME_FORCE_TOL = 2e-5      # relative RMS of dU/dx vs FP64 (FP32 B-splines and FFT)
+PME_REF_FORCE_TOL = 1e-4  # against the reference's FP32 build
+K_ELECTRIC = 332.0716
+
+
+def _pme_case(name):
+    s = CASES[name]()
+    from oracle import pme_oracle
+    K = tuple(pme_oracle.grid_size(L, 1.0) for L in pme_oracle.edge_lengths(s.box6()))
+    return s, K
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("order", [4, 6])
+def test_pme_matches_oracle(cuda, name, order):
+    from oracle import pme_oracle
+    s, K = _pme_case(name)
     nb = NbDirect(s)
-    with pytest.raises(_lib.BnbError, match="unsupported"):
-        nb.set_pme(order=6)
+    nb.set_pme(order=order, grid_space=1.0)
+    assert nb.pme_grid(0) == K
+    f, lf, e = nb.evaluate_pme()
+    lam = s.lambdas() if s.msld else None
+    E, g, L, _ = pme_oracle.pme_recip(s.xyz, s.nbonds["q"], s.box6(), K, order, s.betaEwald, K_ELECTRIC,
+                                      s.nbonds["siteBlock"], lam)
+    assert _rel(f.cpu().numpy(), g) < PME_FORCE_TOL
+    assert float(e.cpu()[0]) == pytest.approx(E, rel=1e-5)
+    if L is not None:
+        assert np.abs(lf.cpu().numpy() - L).max() <= 2e-5 * max(1.0, np.abs(L).max())
     nb.close()
 
 
-GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "tric_*.npz")))
+def test_pme_invariant_under_cell_vector_moves(cuda):
+    s, K = _pme_case("water_tric")
+    ax, bx, by, cx, cy, cz = (float(v) for v in s.tric_box())
+    cellv = np.array([[ax, 0, 0], [bx, by, 0], [cx, cy, cz]])
+    rng = np.random.default_rng(3)
+    moved = s.xyz.astype(np.float64).copy()
+    for w in range(s.N // 3):  # whole waters by random lattice translations
+        moved[3 * w:3 * w + 3] += rng.integers(-2, 3, 3) @ cellv
+    out = []
+    for xyz in (s.xyz, moved.astype(np.float32)):
+        nb = NbDirect(dataclasses.replace(s, xyz=xyz))
+        nb.set_pme(order=6, grid_space=1.0)
+        f, _, e = nb.evaluate_pme()
+        out.append((f.cpu().numpy(), float(e.cpu()[0])))
+        nb.close()
+    assert _rel(out[1][0], out[0][0]) <= 1e-5
+    assert out[1][1] == pytest.approx(out[0][1], rel=1e-5)
+
+
+PME_GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "tric_pme_*.npz")))
+
+
+@pytest.mark.parametrize("path", PME_GOLDEN, ids=[os.path.basename(p)[:-4] for p in PME_GOLDEN])
+def test_pme_matches_reference_triclinic_golden(cuda, path):
+    z = np.load(path)
+    s, K = _pme_case(str(z["case"]))
+    assert np.array_equal(s.xyz, z["xyz"]) and tuple(z["K"]) == K
+    nb = NbDirect(s)
+    nb.set_pme(order=int(z["order"]), grid=K)
+    f, lf, e = nb.evaluate_pme()
+    assert _rel(f.cpu().numpy(), z["grad"].astype(np.float64)) <= PME_REF_FORCE_TOL
+    assert float(e.cpu()[0]) == pytest.approx(float(z["energy"]), rel=1e-5)
+    nb.close()
+
+
+GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "tric_[!p]*.npz")))
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])

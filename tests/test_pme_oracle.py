@@ -112,3 +112,48 @@ def test_total_electrostatics_is_beta_invariant():
         totals.append(sum(parts))
         scale = max(scale, max(abs(p) for p in parts))
     assert abs(totals[0] - totals[1]) < 2e-5 * scale
+
+
+def test_triclinic_converges_to_ewald_sum():
+    """In a triclinic cell (fractional coordinates H^-1 x, k = H^-T m) the
+    restatement converges to the plain Ewald sum over the cell's k vectors."""
+    s = systems.water_box_tric()
+    q = s.nbonds["q"].astype(np.float64)
+    box6 = s.box6()
+    E0, g0 = P.ewald_recip_exact(s.xyz, q, box6, 0.34, K_ELECTRIC, kmax=14)
+    E, g, _, _ = P.pme_recip(s.xyz, q, box6, [64, 48, 64], 8, 0.34, K_ELECTRIC)
+    assert E == pytest.approx(E0, rel=1e-7)
+    assert np.sqrt(((g - g0) ** 2).sum() / (g0 ** 2).sum()) < 1e-6
+
+
+def test_triclinic_orthorhombic_cell_equals_edge_lengths():
+    s = systems.water_box()
+    q = s.nbonds["q"].astype(np.float64)
+    K = [20, 20, 20]
+    E, g, _, _ = P.pme_recip(s.xyz, q, s.box, K, 6, 0.34, K_ELECTRIC)
+    box6 = np.concatenate([np.asarray(s.box, np.float64), np.zeros(3)])
+    E6, g6, _, _ = P.pme_recip(s.xyz, q, box6, K, 6, 0.34, K_ELECTRIC)
+    assert E6 == E and np.array_equal(g6, g)
+    assert np.allclose(P.edge_lengths(box6), s.box)
+
+
+def test_triclinic_finite_differences_and_lattice_moves():
+    s = systems.water_box_tric()
+    q = s.nbonds["q"].astype(np.float64)
+    box6 = s.box6()
+    K = [P.grid_size(L, 1.0) for L in P.edge_lengths(box6)]
+    x0 = s.xyz.astype(np.float64)
+    E, g, _, _ = P.pme_recip(x0, q, box6, K, 6, s.betaEwald, K_ELECTRIC)
+    h = 1e-5
+    for i in (0, 5, 400):
+        for d in range(3):
+            xp = x0.copy(); xp[i, d] += h
+            xm = x0.copy(); xm[i, d] -= h
+            fd = (P.pme_recip(xp, q, box6, K, 6, s.betaEwald, K_ELECTRIC)[0]
+                  - P.pme_recip(xm, q, box6, K, 6, s.betaEwald, K_ELECTRIC)[0]) / (2 * h)
+            assert fd == pytest.approx(g[i, d], rel=1e-5, abs=1e-6)
+    H, _ = P.cell(box6)
+    moved = x0 + np.random.default_rng(2).integers(-2, 3, (len(x0), 3)) @ H.T
+    E2, g2, _, _ = P.pme_recip(moved, q, box6, K, 6, s.betaEwald, K_ELECTRIC)
+    assert E2 == pytest.approx(E, rel=1e-10)
+    assert np.allclose(g2, g, atol=1e-7)

@@ -111,3 +111,30 @@ def test_oracle_matches_reference_triclinic(name):
     if s.msld is not None:
         lf = z["lambdaForce"]
         assert np.abs(o["lambdaForce"][1:] - lf[1:]).max() <= 1e-5 * max(1.0, np.abs(lf).max())
+
+
+@pytest.mark.parametrize("name", GOLDEN)
+def test_pme_oracle_matches_reference_triclinic(name):
+    """The FP64 PME restatement in a triclinic cell against the reference's
+    own triclinic getforce_ewald (flagBox = true with State::kTricBox_f;
+    tests/golden/make_golden.py --tric-pme-only)."""
+    import os
+    import sys
+    from oracle import pme_oracle
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, here)
+    from test_gpu_triclinic import CASES
+    z = np.load(os.path.join(here, "golden", f"tric_pme_{name}.npz"))
+    s = CASES[name]()
+    assert np.array_equal(s.xyz, z["xyz"]) and np.array_equal(s.tric_box(), z["tric_box"])
+    K = [int(k) for k in z["K"]]
+    assert K == [pme_oracle.grid_size(L, 1.0) for L in pme_oracle.edge_lengths(s.box6())]
+    lam = s.lambdas() if s.msld is not None else None
+    E, g, lf, _ = pme_oracle.pme_recip(s.xyz, s.nbonds["q"], s.box6(), K, int(z["order"]), s.betaEwald, 332.0716,
+                                       s.nbonds["siteBlock"], lam)
+    zg = z["grad"].astype(np.float64)
+    assert np.sqrt(((g - zg) ** 2).sum() / (zg ** 2).sum()) <= 1e-5      # the reference computes in FP32
+    assert E == pytest.approx(float(z["energy"]), rel=5e-6)
+    if lf is not None:
+        zl = z["lambdaForce"]
+        assert np.abs(lf[1:] - zl[1:]).max() <= 1e-5 * max(1.0, np.abs(zl).max())
