@@ -96,7 +96,8 @@ struct Counters {
   int workCount;
   int status;
   int workNext;            // dynamic work-item counter of the pair kernel
-  int pad[2];
+  int orderValid;          // Dev::order holds the measured longest-first order of the work items
+  int pad;
   unsigned long long pairCount;
   int levelCount[kWorkLevels];  // work items per level of the work list (rebuild)
   int levelFill[kWorkLevels];   // items written per level (rebuild)
@@ -147,6 +148,8 @@ struct Dev {
   uint32_t *masks;         // [capMask*32]
   int *candStart;          // [maxBlocks+1]
   int2 *work;              // [capWork] (iBlock | tiles << 22, candidate start)
+  unsigned int *itemCost;  // [capWork] clock cycles of each work item in the last pair launch
+  int *order;              // [capWork] work items by decreasing measured cost
   int *scanPartial;        // scratch for multi-CTA scans
   // --- per-step buffers -----------------------------------------------------
   float4 *xyzq;            // [32*maxBlocks]

@@ -55,6 +55,7 @@ struct bnb_handle {
   int tailItems = bnb::kTailItems;
   int smCount = 0;
   bool counting = false;
+  bool orderPending = false;  // sort the work items by cost after the next pair launch
   // profiling (bnb_profile)
   bool prof = false;
   std::vector<cudaEvent_t> pairEv, rebEv;
@@ -202,7 +203,8 @@ int alloc_list(bnb_handle *h) {
   size_t o_cand = a.take<int4>(h->capCand), o_cflag = a.take<int>(h->capCand),
          o_cmo = a.take<int>(h->capCand + 1);
   size_t o_masks = a.take<uint32_t>(32 * (size_t)h->capMask);
-  size_t o_cs = a.take<int>(MB + 1), o_work = a.take<int2>(h->capWork);
+  size_t o_cs = a.take<int>(MB + 1), o_work = a.take<int2>(h->capWork), o_cost = a.take<unsigned int>(h->capWork),
+         o_order = a.take<int>(h->capWork);
   size_t o_part = a.take<int>(4096);
   size_t o_xyzq = a.take<float4>(32 * MB), o_bmin = a.take<float4>(MB), o_bmax = a.take<float4>(MB);
   size_t o_acc = a.take<long long>(3 * 32 * (size_t)MB);
@@ -240,6 +242,8 @@ int alloc_list(bnb_handle *h) {
   d.masks = (uint32_t *)(b + o_masks);
   d.candStart = (int *)(b + o_cs);
   d.work = (int2 *)(b + o_work);
+  d.itemCost = (unsigned int *)(b + o_cost);
+  d.order = (int *)(b + o_order);
   d.scanPartial = (int *)(b + o_part);
   d.xyzq = (float4 *)(b + o_xyzq);
   d.bmin = (float4 *)(b + o_bmin);
@@ -681,6 +685,7 @@ int bnb_rebuild(bnb_handle *h, const float *position, const float *boxes, void *
     const bool rec = h->prof && h->rebN < kProfSlots;
     if (rec) cudaEventRecord(h->rebEv[2 * h->rebN], s);
     h->launches += bnb::rebuild_list(h->d, h->colRep_d, position, rcull2, s);
+    h->orderPending = true;
     if (rec) cudaEventRecord(h->rebEv[2 * h->rebN++ + 1], s);
     if (!ok(cudaGetLastError())) return BNB_ERR_CUDA;
     if (async) {
@@ -767,6 +772,11 @@ int bnb_compute(bnb_handle *h, const float *position, const float *lambda, const
   if (rec) cudaEventRecord(h->pairEv[2 * h->pairN++ + 1], s);
   if (rc) return rc;
   bnb::launch_finalize(h->d, *out, out_mode(calcEnergy), s);
+  if (h->orderPending) {  // the costs of this launch order the items of the next ones
+    bnb::launch_order(h->d, s);
+    h->orderPending = false;
+    h->launches += 1;
+  }
   h->launches += 3;
   return ok(cudaGetLastError()) ? BNB_OK : BNB_ERR_CUDA;
 }

@@ -296,6 +296,7 @@ __global__ void k_colscan(Dev d, const int *__restrict__ colRep) {
     d.ctr->levelCount[threadIdx.x] = 0;
     d.ctr->levelFill[threadIdx.x] = 0;
   }
+  if (threadIdx.x == 0) d.ctr->orderValid = 0;  // until the new items are measured
   __syncthreads();
   for (int r = threadIdx.x; r <= d.R; r += blockDim.x) {
     int b = r < d.R ? d.colStartBlock[d.rep[r].colStart] : d.colStartBlock[nc];

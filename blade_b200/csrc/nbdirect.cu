@@ -582,11 +582,16 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
   const int S = 32 * d.maxBlocks;
   unsigned long long pairs = 0;
 
-  int w = 0;
+  // after the first launch of a list the items are taken longest first, in
+  // the order their measured cycles gave (launch_order)
+  const bool ordered = d.ctr->orderValid != 0;
+  int w = 0;  // position in this launch's sequence of items
   if (lane == 0) w = atomicAdd(&d.ctr->workNext, 1);
   w = __shfl_sync(kFull, w, 0);
   while (w < nWork) {
-    const int2 wk = d.work[w];
+    const int item = ordered ? d.order[w] : w;
+    const long long tItem = clock64();
+    const int2 wk = d.work[item];
     const int iBlock = wk.x & 0x3FFFFF;
     const int c0 = wk.y;
     int c1 = d.candStart[iBlock + 1];
@@ -853,7 +858,11 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
       for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(kFull, e, o);
       if (lane == 0 && e != 0) red_add(&d.accE[d.blockRep[iBlock]], e);
     }
-    if (lane == 0) w = atomicAdd(&d.ctr->workNext, 1);
+    if (lane == 0) {
+      const long long dt = clock64() - tItem;
+      d.itemCost[item] = dt < 0xFFFFFFFFll ? (unsigned int)dt : 0xFFFFFFFFu;
+      w = atomicAdd(&d.ctr->workNext, 1);
+    }
     w = __shfl_sync(kFull, w, 0);
   }
   if (A.count) {
@@ -866,6 +875,52 @@ __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
     for (int i = threadIdx.x; i < d.lamTotal; i += blockDim.x)
       if (sAccL[i]) red_add(&d.accL[i], sAccL[i]);
   }
+}
+
+// Log-scale bucket of a cycle count: 8 buckets per octave, 0..255.
+__device__ __forceinline__ int cost_bucket(unsigned int c) {
+  c = c ? c : 1u;
+  const int e = 31 - __clz(c);
+  const int m = e >= 3 ? (int)(c >> (e - 3)) & 7 : (int)(c << (3 - e)) & 7;
+  return 8 * e + m;
+}
+
+// Work items by decreasing measured cost, one CTA: a histogram of the costs
+// in log-scale buckets, bucket offsets from the most expensive bucket down
+// (a warp scan over 256 buckets), then every item placed in its bucket.
+// Inside a bucket the order follows the shared-memory atomics; the results
+// of the pair kernel do not depend on the order of its items.
+__global__ void __launch_bounds__(1024) k_order(Dev d) {
+  __shared__ int hist[256];
+  const int n = (d.ctr->status & kStatusListInvalid) ? 0 : d.ctr->workCount;
+  for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&hist[cost_bucket(d.itemCost[i])], 1);
+  __syncthreads();
+  if (threadIdx.x < 32) {  // lane l owns buckets 255 - 8l .. 248 - 8l (descending)
+    const int l = threadIdx.x;
+    int c[8], sum = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      c[k] = hist[255 - 8 * l - k];
+      sum += c[k];
+    }
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(kFull, incl, o);
+      if (l >= o) incl += v;
+    }
+    int run = incl - sum;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      hist[255 - 8 * l - k] = run;
+      run += c[k];
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) d.order[atomicAdd(&hist[cost_bucket(d.itemCost[i])], 1)] = i;
+  if (threadIdx.x == 0) d.ctr->orderValid = n > 0;
 }
 
 // Converts the fixed-point accumulators to the caller's outputs and clears them.
@@ -1100,6 +1155,8 @@ void launch_finalize(const Dev &d, const bnb_outputs &o, int mode, cudaStream_t 
   if (grid < 1) grid = 1;
   k_finalize<<<grid, 256, 0, s>>>(d, o, mode);
 }
+
+void launch_order(const Dev &d, cudaStream_t s) { k_order<<<1, 1024, 0, s>>>(d); }
 
 int launch_allpairs(const AllPairsArgs &a, const bnb_outputs &o, int elec, int vdw, bool energy,
                     cudaStream_t s) {

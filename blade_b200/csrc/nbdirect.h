@@ -9,6 +9,10 @@ namespace bnb {
 int launch_pair(const Dev &d, const PairConst &pc, const float *lambda, int elec, int vdw,
                 int alch, bool energy, bool count, int grid, cudaStream_t s);
 void launch_finalize(const Dev &d, const bnb_outputs &o, int mode, cudaStream_t s);
+// Sorts the work items by the cycles the last pair launch measured for them,
+// longest first, into Dev::order, which the following launches follow until
+// the next rebuild; one launch.
+void launch_order(const Dev &d, cudaStream_t s);
 
 // All-pairs evaluation of one small system (bnb_nbdirect_noalloc).  accF is
 // [3 * stride] (component planes), accE one entry; both must be zero on
