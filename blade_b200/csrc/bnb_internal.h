@@ -12,6 +12,8 @@
 #include "bnb.h"
 #include "work_split.h"
 
+#include <utility>
+
 namespace bnb {
 
 constexpr int kNumShifts = 14;        // own image + 13 half-shell images
@@ -176,5 +178,35 @@ struct PairConst {        // uniform parameters of the pair kernel
   float fsG, fsG5, fsC1, fsP1, fsP2, fsP3;   // factored FSWITCH (see pair_terms)
   float vshRc6inv, vshRc12inv, vshRc18inv;
 };
+
+// Programmatic dependent launch for the kernels of the list rebuild and the
+// per-step path: each is launched with programmatic stream serialization, so
+// its launch (and the scheduling of its CTAs) overlaps the end of the kernel
+// before it in the stream instead of following it; every such kernel calls
+// pdl_wait() before it touches device memory, which returns once the kernel
+// before it has completed and its writes are visible.  Since each kernel
+// waits for its predecessor, the stream keeps its order transitively.  A
+// kernel launched without the attribute returns from pdl_wait() at once.
+__device__ __forceinline__ void pdl_wait() {
+#if defined(__CUDA_ARCH__)
+  cudaGridDependencySynchronize();
+#endif
+}
+
+template <typename... P, typename... A>
+inline cudaError_t launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              A &&...args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
 
 }  // namespace bnb

@@ -87,6 +87,7 @@ __device__ int block_excl_scan(int v, int *total) {
 }
 
 __global__ void k_scan_reduce(const int *in, int n, int *partial) {
+  pdl_wait();
   int base = blockIdx.x * kScanTile;
   int s = 0;
   for (int i = threadIdx.x; i < kScanTile; i += kScanThreads) {
@@ -99,6 +100,7 @@ __global__ void k_scan_reduce(const int *in, int n, int *partial) {
 }
 
 __global__ void k_scan_top(int *partial, int nParts, int *total) {
+  pdl_wait();
   // nParts <= kScanTile
   int v[kScanItems];
   int s = 0;
@@ -120,6 +122,7 @@ __global__ void k_scan_top(int *partial, int nParts, int *total) {
 }
 
 __global__ void k_scan_down(const int *in, int *out, int n, const int *partial) {
+  pdl_wait();
   int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
   int v[kScanItems];
   int s = 0;
@@ -141,6 +144,7 @@ __global__ void k_scan_down(const int *in, int *out, int n, const int *partial) 
 
 // Small arrays: one CTA walks the array tile by tile with a running carry.
 __global__ void k_scan_single(const int *in, int *out, int n, int *total) {
+  pdl_wait();
   __shared__ int carry;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
@@ -172,14 +176,14 @@ __global__ void k_scan_single(const int *in, int *out, int n, int *total) {
 int scan_exclusive(const int *in, int *out, int n, int *total, int *partial,
                    cudaStream_t s) {
   if (n <= 4 * kScanTile) {  // up to 16,384 items: one launch instead of three
-    k_scan_single<<<1, kScanThreads, 0, s>>>(in, out, n, total);
+    launch_pdl(k_scan_single, 1, kScanThreads, 0, s, in, out, n, total);
     return 1;
   }
   int parts = (n + kScanTile - 1) / kScanTile;
   if (parts < 1) parts = 1;
-  k_scan_reduce<<<parts, kScanThreads, 0, s>>>(in, n, partial);
-  k_scan_top<<<1, kScanThreads, 0, s>>>(partial, parts, total);
-  k_scan_down<<<parts, kScanThreads, 0, s>>>(in, out, n, partial);
+  launch_pdl(k_scan_reduce, parts, kScanThreads, 0, s, in, n, partial);
+  launch_pdl(k_scan_top, 1, kScanThreads, 0, s, partial, parts, total);
+  launch_pdl(k_scan_down, parts, kScanThreads, 0, s, in, out, n, partial);
   return 3;
 }
 
@@ -189,6 +193,7 @@ namespace {
 // 1. Binning: wrap shift, column and z key per atom.
 // ---------------------------------------------------------------------------
 __global__ void k_bin(Dev d, const float *__restrict__ pos) {
+  pdl_wait();
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a == 0) atomicAnd(&d.ctr->status, ~kStatusListInvalid);  // this rebuild starts a fresh list
   if (a >= d.N) return;
@@ -228,6 +233,7 @@ __global__ void k_bin(Dev d, const float *__restrict__ pos) {
 // 2. Column scan (single CTA): atom offsets, block offsets, block bounds.
 // ---------------------------------------------------------------------------
 __global__ void k_colscan(Dev d, const int *__restrict__ colRep) {
+  pdl_wait();
   __shared__ int carryA, carryB;
   if (threadIdx.x == 0) { carryA = 0; carryB = 0; }
   __syncthreads();
@@ -306,6 +312,7 @@ __global__ void k_colscan(Dev d, const int *__restrict__ colRep) {
 
 // 3. Scatter atoms into column buckets (arbitrary order within a column).
 __global__ void k_scatter(Dev d) {
+  pdl_wait();
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= d.N) return;
   int col = d.atomCol[a];
@@ -316,6 +323,7 @@ __global__ void k_scatter(Dev d) {
 // 4. Sort each column by (z key, atom index): bitonic sort in shared memory,
 //    rank counting for columns larger than kSortCap.
 __global__ void k_colsort(Dev d) {
+  pdl_wait();
   __shared__ unsigned long long key[kSortCap];
   const int c = blockIdx.x;
   const int n = d.colCount[c];
@@ -367,6 +375,7 @@ __global__ void k_colsort(Dev d) {
 
 // 5. Slots: atom of each of the 32 lanes of each block, per-slot parameters.
 __global__ void k_slots(Dev d) {
+  pdl_wait();
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   int b = t >> 5, lane = t & 31;
   if (b >= d.maxBlocks) return;
@@ -400,6 +409,7 @@ __global__ void k_slots(Dev d) {
 //    reproducible).  A block that hits implies its column hits under the
 //    rounding of aabb_hit, so the cull may skip columns that miss.
 __global__ void k_pack(Dev d, const float *__restrict__ pos, bool columns) {
+  pdl_wait();
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   int b = t >> 5;
   if (b >= d.maxBlocks) return;
@@ -458,6 +468,7 @@ __device__ __forceinline__ float key_float(uint32_t k) {
 //      the candidates come out in the order of a scan over all j blocks.
 template <bool kWrite>
 __global__ void k_cull(Dev d, float rcull2) {
+  pdl_wait();
   const int lane = threadIdx.x & 31;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
   const int B = d.ctr->blockCount;
@@ -565,6 +576,7 @@ __device__ __forceinline__ uint32_t excl_row(const Dev &d, int iBlock, int jBloc
 //      k_excl skips their per-atom scan.  More than kExclBlk blocks: count -1,
 //      and every tile of the block takes the full scan.
 __global__ void k_excl_blocks(Dev d) {
+  pdl_wait();
   __shared__ int sList[8][kExclBlk];
   const int lane = threadIdx.x & 31;
   const int warp = (threadIdx.x >> 5) & 7;
@@ -605,6 +617,7 @@ __global__ void k_excl_blocks(Dev d) {
 
 template <bool kWrite>
 __global__ void k_excl(Dev d) {
+  pdl_wait();
   const int lane = threadIdx.x & 31;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
   const int n = d.ctr->candCount;
@@ -648,6 +661,7 @@ __global__ void k_excl(Dev d) {
 //     warps finish close together.  Within a level the order follows the
 //     atomics; the items themselves depend on their block only.
 __global__ void k_work(Dev d) {
+  pdl_wait();
   const int B = d.ctr->blockCount;
   int off[kWorkLevels + 1];
   off[0] = 0;
@@ -681,42 +695,45 @@ inline int grid_for(long long n, int threads) {
 
 void pack_positions(const Dev &d, const float *pos, cudaStream_t s) {
   int n = 32 * d.maxBlocks;
-  k_pack<<<grid_for(n, 256), 256, 0, s>>>(d, pos, false);
+  launch_pdl(k_pack, grid_for(n, 256), 256, 0, s, d, pos, false);
 }
 
 namespace {
-__global__ void k_clear_status(Counters *c) { atomicAnd(&c->status, ~kStatusListInvalid); }
+__global__ void k_clear_status(Counters *c) {
+  pdl_wait();
+  atomicAnd(&c->status, ~kStatusListInvalid);
+}
 }  // namespace
 
 int rebuild_list(const Dev &d, const int *colRep, const float *pos, float rcull2,
                  cudaStream_t s) {
   int launches = 8;  // bin or clear, colscan, colsort, slots, pack, excl_blocks, work, + scatter or not below
   // colCount is zero here: set so at allocation and by k_colsort after use
-  if (d.N > 0) k_bin<<<grid_for(d.N, 256), 256, 0, s>>>(d, pos);  // also clears the list-invalid bits
-  else k_clear_status<<<1, 1, 0, s>>>(d.ctr);
-  k_colscan<<<1, 1024, 0, s>>>(d, colRep);
+  if (d.N > 0) launch_pdl(k_bin, grid_for(d.N, 256), 256, 0, s, d, pos);  // also clears the list-invalid bits
+  else launch_pdl(k_clear_status, 1, 1, 0, s, d.ctr);
+  launch_pdl(k_colscan, 1, 1024, 0, s, d, colRep);
   if (d.N > 0) {
-    k_scatter<<<grid_for(d.N, 256), 256, 0, s>>>(d);
+    launch_pdl(k_scatter, grid_for(d.N, 256), 256, 0, s, d);
     launches++;
   }
-  k_colsort<<<d.totalCols, 512, 0, s>>>(d);
-  k_slots<<<grid_for(32LL * d.maxBlocks, 256), 256, 0, s>>>(d);
-  k_pack<<<grid_for(32LL * d.maxBlocks, 256), 256, 0, s>>>(d, pos, true);
-  k_excl_blocks<<<grid_for(32LL * d.maxBlocks, 256), 256, 0, s>>>(d);
+  launch_pdl(k_colsort, d.totalCols, 512, 0, s, d);
+  launch_pdl(k_slots, grid_for(32LL * d.maxBlocks, 256), 256, 0, s, d);
+  launch_pdl(k_pack, grid_for(32LL * d.maxBlocks, 256), 256, 0, s, d, pos, true);
+  launch_pdl(k_excl_blocks, grid_for(32LL * d.maxBlocks, 256), 256, 0, s, d);
   // cull: count, scan, write
   const int cullWarps = d.maxBlocks * kNumShifts;
   const int cullGrid = grid_for(32LL * cullWarps, 256) < 148 * 32 ? grid_for(32LL * cullWarps, 256) : 148 * 32;
-  k_cull<false><<<cullGrid, 256, 0, s>>>(d, rcull2);
+  launch_pdl(k_cull<false>, cullGrid, 256, 0, s, d, rcull2);
   launches += 4;  // two cull and two exclusion passes
   launches += scan_exclusive(d.cullCount, d.cullOffset, cullWarps, d.cullOffset + cullWarps, d.scanPartial, s);
-  k_cull<true><<<cullGrid, 256, 0, s>>>(d, rcull2);  // also candStart, work counts, candCount
+  launch_pdl(k_cull<true>, cullGrid, 256, 0, s, d, rcull2);  // also candStart, work counts, candCount
   // exclusion masks: flag, scan, write
   const int exGrid = grid_for(32LL * d.capCand, 256) < 148 * 16 ? grid_for(32LL * d.capCand, 256) : 148 * 16;
-  k_excl<false><<<exGrid, 256, 0, s>>>(d);
+  launch_pdl(k_excl<false>, exGrid, 256, 0, s, d);
   launches += scan_exclusive(d.candFlag, d.candMaskOff, d.capCand, d.candMaskOff + d.capCand, d.scanPartial, s);
-  k_excl<true><<<exGrid, 256, 0, s>>>(d);  // also maskCount
+  launch_pdl(k_excl<true>, exGrid, 256, 0, s, d);  // also maskCount
   // work items
-  k_work<<<grid_for(d.maxBlocks, 256), 256, 0, s>>>(d);
+  launch_pdl(k_work, grid_for(d.maxBlocks, 256), 256, 0, s, d);
   return launches;
 }
 

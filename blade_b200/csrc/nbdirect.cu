@@ -551,6 +551,7 @@ __device__ __forceinline__ void stream_round(const Dev &d, const PairConst &pc, 
 // ---------------------------------------------------------------------------
 template <int ELEC, int VDW, int ALCH, bool ENERGY, bool COMBINE>
 __global__ void __launch_bounds__(256, 2) k_pair(KArgs A) {
+  pdl_wait();
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int sIdx[8][32];
   __shared__ int sStream[8][128];  // queued entries of streamed tiles, per warp
@@ -891,6 +892,7 @@ __device__ __forceinline__ int cost_bucket(unsigned int c) {
 // Inside a bucket the order follows the shared-memory atomics; the results
 // of the pair kernel do not depend on the order of its items.
 __global__ void __launch_bounds__(1024) k_order(Dev d) {
+  pdl_wait();
   __shared__ int hist[256];
   const int n = (d.ctr->status & kStatusListInvalid) ? 0 : d.ctr->workCount;
   for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0;
@@ -928,6 +930,7 @@ __global__ void __launch_bounds__(1024) k_order(Dev d) {
 // order) are written coalesced, and the per-slot accumulators, still in L2
 // from the pair kernel's atomics, are gathered through atomSlot.
 __global__ void k_finalize(Dev d, bnb_outputs o, int mode) {
+  pdl_wait();
   const int S = 32 * d.maxBlocks;
   const double inv = 1.0 / kFixScale;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < d.N; a += gridDim.x * blockDim.x) {
@@ -979,7 +982,7 @@ void launch_t(const KArgs &a, int maxGrid, size_t shmem, cudaStream_t s) {
   int grid = perSM * sms;
   if (grid > maxGrid) grid = maxGrid;
   if (grid < 1) grid = 1;
-  k<<<grid, 256, shmem, s>>>(a);
+  launch_pdl(k, grid, 256, shmem, s, a);
 }
 
 template <int ELEC, int VDW>
@@ -1153,10 +1156,10 @@ void launch_finalize(const Dev &d, const bnb_outputs &o, int mode, cudaStream_t 
   int grid = (n + 255) / 256;
   if (grid > 148 * 8) grid = 148 * 8;
   if (grid < 1) grid = 1;
-  k_finalize<<<grid, 256, 0, s>>>(d, o, mode);
+  launch_pdl(k_finalize, grid, 256, 0, s, d, o, mode);
 }
 
-void launch_order(const Dev &d, cudaStream_t s) { k_order<<<1, 1024, 0, s>>>(d); }
+void launch_order(const Dev &d, cudaStream_t s) { launch_pdl(k_order, 1, 1024, 0, s, d); }
 
 int launch_allpairs(const AllPairsArgs &a, const bnb_outputs &o, int elec, int vdw, bool energy,
                     cudaStream_t s) {
