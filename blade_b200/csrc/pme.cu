@@ -142,6 +142,7 @@ __device__ __forceinline__ float atom_scale(const PmeArgs &a, int atom, int &blo
 // ---------------------------------------------------------------------------
 template <int ORDER>
 __global__ void __launch_bounds__(256) k_spread(PmeArgs a) {
+  pdl_wait();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int atom = t >> 3, g = t & 7;
   if (atom >= a.N || g >= ORDER) return;
@@ -182,6 +183,7 @@ __global__ void __launch_bounds__(256) k_spread(PmeArgs a) {
 
 // Fixed point -> FP32 grid, clearing the fixed-point grid for the next call.
 __global__ void k_fix_to_grid(PmeArgs a) {
+  pdl_wait();
   const double inv = 1.0 / kFixScale;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.totalGrid; i += gridDim.x * blockDim.x) {
     const long long v = a.qfix[i];
@@ -195,6 +197,7 @@ __global__ void k_fix_to_grid(PmeArgs a) {
 // FP32 like the reference's kernel (nbrecip.cu:215-256).
 // ---------------------------------------------------------------------------
 __global__ void k_convolve(PmeArgs a) {
+  pdl_wait();
   const int r = blockIdx.y;
   const PmeRep pr = a.prep[r];
   const RepInfo &ri = a.rep[r];
@@ -272,6 +275,7 @@ __device__ void finalize_if_last(const PmeArgs &a, const bnb_outputs &o, bool en
 // ---------------------------------------------------------------------------
 template <int ORDER, bool ENERGY>
 __global__ void __launch_bounds__(256) k_gather(PmeArgs a, bnb_outputs o) {
+  pdl_wait();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const int atom = t >> 3, g = t & 7;
@@ -383,6 +387,7 @@ __global__ void __launch_bounds__(256) k_gather(PmeArgs a, bnb_outputs o) {
 // ---------------------------------------------------------------------------
 template <bool ENERGY>
 __global__ void k_self(PmeArgs a, float pre, bnb_outputs o) {
+  pdl_wait();
   const int lane = threadIdx.x & 31;
   const int atom = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = atom < a.N;
@@ -413,7 +418,10 @@ __global__ void k_self(PmeArgs a, float pre, bnb_outputs o) {
 }
 
 // lambda and energy accumulators -> outputs when there are no atoms (one CTA).
-__global__ void k_pme_finalize(PmeArgs a, bnb_outputs o, bool energy) { finalize_outputs(a, o, energy); }
+__global__ void k_pme_finalize(PmeArgs a, bnb_outputs o, bool energy) {
+  pdl_wait();
+  finalize_outputs(a, o, energy);
+}
 
 inline int grid_of(long long threads, int block) {
   long long g = (threads + block - 1) / block;
@@ -426,20 +434,20 @@ int pme_spread(const PmeArgs &a, cudaStream_t s) {
   if (a.N > 0) {
     const int grid = (int)((8LL * a.N + 255) / 256);
     switch (a.order) {
-      case 4: k_spread<4><<<grid, 256, 0, s>>>(a); break;
-      case 6: k_spread<6><<<grid, 256, 0, s>>>(a); break;
-      case 8: k_spread<8><<<grid, 256, 0, s>>>(a); break;
+      case 4: launch_pdl(k_spread<4>, grid, 256, 0, s, a); break;
+      case 6: launch_pdl(k_spread<6>, grid, 256, 0, s, a); break;
+      case 8: launch_pdl(k_spread<8>, grid, 256, 0, s, a); break;
       default: return BNB_ERR_ARG;
     }
   }
-  k_fix_to_grid<<<grid_of(a.totalGrid, 256), 256, 0, s>>>(a);
+  launch_pdl(k_fix_to_grid, grid_of(a.totalGrid, 256), 256, 0, s, a);
   return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
 }
 
 int pme_convolve(const PmeArgs &a, cudaStream_t s) {
   int gx = (a.maxCplx + 1023) / 1024;  // about 4 elements per thread
   gx = gx < 1 ? 1 : gx;
-  k_convolve<<<dim3(gx, a.R), 256, 0, s>>>(a);
+  launch_pdl(k_convolve, dim3(gx, a.R), 256, 0, s, a);
   return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
 }
 
@@ -447,16 +455,16 @@ int pme_gather(const PmeArgs &a, const bnb_outputs &o, bool energy, cudaStream_t
   if (a.N > 0) {
     const int grid = (int)((8LL * a.N + 255) / 256);
     switch (a.order * 2 + (energy ? 1 : 0)) {
-      case 8: k_gather<4, false><<<grid, 256, 0, s>>>(a, o); break;
-      case 9: k_gather<4, true><<<grid, 256, 0, s>>>(a, o); break;
-      case 12: k_gather<6, false><<<grid, 256, 0, s>>>(a, o); break;
-      case 13: k_gather<6, true><<<grid, 256, 0, s>>>(a, o); break;
-      case 16: k_gather<8, false><<<grid, 256, 0, s>>>(a, o); break;
-      case 17: k_gather<8, true><<<grid, 256, 0, s>>>(a, o); break;
+      case 8: launch_pdl(k_gather<4, false>, grid, 256, 0, s, a, o); break;
+      case 9: launch_pdl(k_gather<4, true>, grid, 256, 0, s, a, o); break;
+      case 12: launch_pdl(k_gather<6, false>, grid, 256, 0, s, a, o); break;
+      case 13: launch_pdl(k_gather<6, true>, grid, 256, 0, s, a, o); break;
+      case 16: launch_pdl(k_gather<8, false>, grid, 256, 0, s, a, o); break;
+      case 17: launch_pdl(k_gather<8, true>, grid, 256, 0, s, a, o); break;
       default: return BNB_ERR_ARG;
     }
   } else {
-    k_pme_finalize<<<1, 256, 0, s>>>(a, o, energy);
+    launch_pdl(k_pme_finalize, 1, 256, 0, s, a, o, energy);
   }
   return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
 }
@@ -466,10 +474,10 @@ int pme_self(const PmeArgs &a, const bnb_outputs &o, bool energy, cudaStream_t s
   const float pre = (float)(-(double)a.beta / sqrt(kPi));
   if (a.N > 0) {
     const int grid = (a.N + 255) / 256;
-    if (energy) k_self<true><<<grid, 256, 0, s>>>(a, pre, o);
-    else k_self<false><<<grid, 256, 0, s>>>(a, pre, o);
+    if (energy) launch_pdl(k_self<true>, grid, 256, 0, s, a, pre, o);
+    else launch_pdl(k_self<false>, grid, 256, 0, s, a, pre, o);
   } else {
-    k_pme_finalize<<<1, 256, 0, s>>>(a, o, energy);
+    launch_pdl(k_pme_finalize, 1, 256, 0, s, a, o, energy);
   }
   return cudaGetLastError() == cudaSuccess ? BNB_OK : BNB_ERR_CUDA;
 }
