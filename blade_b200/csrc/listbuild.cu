@@ -626,6 +626,10 @@ __global__ void k_excl(Dev d) {
       if (!kWrite && lane == 0) d.candFlag[c] = 0;
       continue;
     }
+    if (kWrite && d.candMaskOff[c + 1] == d.candMaskOff[c]) {  // the flag pass found no exclusion here
+      if (lane == 0) d.cand[c].z = -1;
+      continue;
+    }
     int4 t = d.cand[c];
     const int nb = d.exclBlkCount[t.w];
     bool scan = true;
@@ -672,15 +676,26 @@ __global__ void k_work(Dev d) {
     d.ctr->workCount = total < d.capWork ? total : d.capWork;
     if (total > d.capWork) atomicOr(&d.ctr->status, kStatusWorkOverflow);
   }
-  for (int b = t; b < B; b += gridDim.x * blockDim.x) {
+  // one warp per block: lane 0 reserves each level's items, the lanes write them
+  const int lane = threadIdx.x & 31, nWarps = (gridDim.x * blockDim.x) >> 5;
+  for (int b = t >> 5; b < B; b += nWarps) {
     const int c0 = d.candStart[b], nc = d.candStart[b + 1] - c0;
     int tiles[kWorkLevels], items[kWorkLevels];
-    work_split(nc, d.tilesPerWork, d.tailTiles, tiles, items);
-    int base = 0;
-    work_walk(c0, nc, d.tilesPerWork, d.tailTiles, [&](int l, int k, int first, int n) {
-      if (k == 0) base = off[l] + atomicAdd(&d.ctr->levelFill[l], items[l]);
-      if (base + k < d.capWork) d.work[base + k] = make_int2(b | (n << 22), first);
-    });
+    const int L = work_split(nc, d.tilesPerWork, d.tailTiles, tiles, items);
+    int s = c0;  // first candidate of the level (the order of work_walk)
+    for (int l = 0; l < L; l++) {
+      const int size = work_item_size(d.tilesPerWork, l), end = s + tiles[l];
+      if (items[l]) {
+        int base = 0;
+        if (lane == 0) base = off[l] + atomicAdd(&d.ctr->levelFill[l], items[l]);
+        base = __shfl_sync(kFull, base, 0);
+        for (int k = lane; k < items[l]; k += 32) {
+          const int first = s + k * size, n = end - first < size ? end - first : size;
+          if (base + k < d.capWork) d.work[base + k] = make_int2(b | (n << 22), first);
+        }
+      }
+      s = end;
+    }
   }
 }
 
@@ -733,7 +748,7 @@ int rebuild_list(const Dev &d, const int *colRep, const float *pos, float rcull2
   launches += scan_exclusive(d.candFlag, d.candMaskOff, d.capCand, d.candMaskOff + d.capCand, d.scanPartial, s);
   launch_pdl(k_excl<true>, exGrid, 256, 0, s, d);  // also maskCount
   // work items
-  launch_pdl(k_work, grid_for(d.maxBlocks, 256), 256, 0, s, d);
+  launch_pdl(k_work, grid_for(32LL * d.maxBlocks, 256), 256, 0, s, d);
   return launches;
 }
 
