@@ -451,6 +451,9 @@ def run_bnb(args, rank, world):
         "config": {"workload": WORKLOADS[args.workload][0], "atoms": s.N, "lj_types": s.nTypes, "pairs_per_step": P / K, "jitter_A": JITTER,
                    "energy_every": ENERGY_EVERY,
                    "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}",
+                   "outputs": "dU/dx added to a device FP32 force array and the energy to an FP64 one "
+                              "(the reference's semantics: atomic adds in the finalize); the e2e leg "
+                              "overwrites its outputs (BNB_OUT_SET) and copies them to the host",
                    "tuning": tuning},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_t, "unit": "TFLOP/s",
                      "frac": achieved / peak_t, "traffic": traffic,
