@@ -470,18 +470,19 @@ __device__ __forceinline__ void stream_round(const Dev &d, const PairConst &pc, 
   float jfx = 0.f, jfy = 0.f, jfz = 0.f;
 #pragma unroll 2
   for (int k = 0; k < gw; k++) {
-    const float2 dx = make_float2(I.x.x - jx, I.x.y - jx);
-    const float2 dy = make_float2(I.y.x - jy, I.y.y - jy);
-    const float2 dz = make_float2(I.z.x - jz, I.z.y - jz);
+    // packed operations with the j value replicated into both halves
+    const float2 dx = fma2(f2(jx), f2(-1.f), I.x);
+    const float2 dy = fma2(f2(jy), f2(-1.f), I.y);
+    const float2 dz = fma2(f2(jz), f2(-1.f), I.z);
     const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
     const bool actA = r2.x < pc.rc2, actB = r2.y < pc.rc2;
-    const float2 qq = make_float2(I.q.x * jq, I.q.y * jq);
+    const float2 qq = mul2(I.q, f2(jq));
     float2 fs, E = f2(0.f);
     if (ELEC == 1 && VDW == 0) {
       float2 lj0, lj1;
       if (COMBINE) {
-        lj0 = make_float2(I.e6.x * jex, I.e6.y * jex);
-        lj1 = make_float2(I.R.x + jer, I.R.y + jer);
+        lj0 = mul2(I.e6, f2(jex));
+        lj1 = add2(I.R, f2(jer));
       } else {
         const float2 vA = sLJ[I.rowA + tj], vB = sLJ[I.rowB + tj];
         lj0 = make_float2(vA.x, vB.x);
