@@ -4,20 +4,30 @@
 // plus recull_blocks (src/domdec/recull.cu:41-122) and unpack_forces
 // (src/domdec/assign_blocks.cu:444-468), redesigned for Blackwell SIMT:
 //
-//  * Work item = one i-block x up to tilesPerWork candidate j-tiles.  A warp
+//  * Work item = one i-block x up to 32 candidate j-tiles (the list rebuild
+//    splits each block's candidates into items, work_split.h).  A warp
 //    recull-tests its candidates at rCut with the fresh AABBs (one lane per
-//    candidate, ballot), then walks the surviving tiles.
-//  * j-tile rotation: lane l owns i-atom l for the whole work item and holds
-//    j-atom (l+k)&31 at step k.  After each step the j coordinates, charge,
-//    type and the j-force accumulators move one lane down with __shfl_sync, so
-//    after 32 steps every j-force is back in its owner lane and no butterfly
-//    reduction is needed (the reference spends 15 xor-shuffles per j atom).
+//    candidate, ballot), then walks the surviving tiles; the persistent warps
+//    pull items from a counter, longest first once a launch has measured
+//    their cycles (k_order).
+//  * Tiles without exclusion mask and MSLD atom are streamed: their j atoms
+//    that can reach the i block are queued per warp and evaluated in rounds
+//    in which each lane holds two i atoms and one j atom, the pair math of
+//    the two pairs in packed FP32x2 instructions, the j atom (coordinates,
+//    charge, LJ parameters, force) rotating through a group of lanes with
+//    __shfl_sync, so every j force returns to its lane without a butterfly
+//    reduction (the reference spends 15 xor-shuffles per j atom).
+//  * Masked and MSLD tiles are evaluated per tile: lane l owns i atom l and
+//    the compacted j atoms rotate through groups of 32, 16, 8 or 4 lanes.
 //  * Accumulation in int64 fixed point (2^-32 units): i forces once per work
-//    item, j forces once per tile, energy and dU/dlambda per work item.  The
-//    FP32 partial sums inside a work item have a fixed order, so results do
-//    not depend on which warp, CTA or launch runs which work item.
+//    item, j forces once per queued atom or tile chunk, energy per pair and
+//    dU/dlambda per work item.  The FP32 partial sums inside a work item have
+//    a fixed order, so results do not depend on which warp, CTA or launch
+//    runs which work item, nor on the order in which the items are taken.
 //  * Pair math in FP32: rsqrt, erfc as exp(-x^2)*P6(1/(1+p x)) sharing the
 //    Gaussian with the force (erfc_fit.h), branch-free force switching.
+//  * Launched with programmatic dependent launch (launch_pdl): each kernel
+//    waits for its predecessor in pdl_wait() before touching memory.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
