@@ -182,6 +182,39 @@ def site_flatness(sm: SiteMap, hist1, end_count):
     return dev, frac
 
 
+def site_flatness_pooled(sm: SiteMap, recs, window: int, T: float = 300.0):
+    """Per site: (deviation of the end-state populations from uniform, fraction
+    of samples at an end state) from the last ``window`` iterations of
+    ``recs`` pooled, each iteration's end-state counts reweighted to the
+    parameters of the last one.  At an end state of a site (lambda_i = 1, the
+    others 0) only the fixed bias b_i of that substituent acts -- the c, x and
+    s terms vanish there -- so counts gathered under b' reweight to b by
+    exp(-(b_i - b'_i) / kT) exactly; pooling several short runs lowers the
+    sampling noise of the judgement."""
+    kT = KB * T
+    recs = recs[-window:]
+    last = recs[-1]["params"]
+    dev = np.zeros(len(sm.sites))
+    frac = np.zeros(len(sm.sites))
+    for k, g in enumerate(sm.sites):
+        n = len(g)
+        o = sm.param_offset[k]
+        c = np.zeros(n)
+        ends = samples = 0.0
+        for r in recs:
+            cnt = r["he"][g].astype(np.float64)
+            shift = last[o:o + n] - r["params"][o:o + n]
+            num = cnt * np.exp(-(shift - shift.min()) / kT)   # the common factor cancels
+            if num.sum() > 0:                                 # this run's populations under the last
+                c += cnt.sum() * num / num.sum()              # biases, weighted by its end samples
+            ends += cnt.sum()
+            samples += max(1, int(r["h1"][g[0]].sum()))
+        tot = c.sum()
+        dev[k] = float(np.abs(c / tot - 1.0 / n).max()) if tot > 0 else 1.0 - 1.0 / n
+        frac[k] = ends / samples
+    return dev, frac
+
+
 def plain_update(sm: SiteMap, hist1, hist2, end_count, T: float = 300.0) -> np.ndarray:
     """The plain flattening update (change of every parameter) from one
     iteration's histograms, site by site:
@@ -529,12 +562,14 @@ def site_iterations_to_flat(recs_dev_frac) -> np.ndarray:
 
 
 def run_sites(drv: AlfBatch, n_iter: int, model=None, scale: float = 1.0, with_plain: bool = False,
-              learned_iters: int | None = None):
+              learned_iters: int | None = None, pool: int = 0):
     """n_iter iterations of plain (model None) or learned flattening; returns
     per-iteration records with per-site flatness and whether the plain
     fallback was used.  The learned step is ``scale`` times the predicted
     lookahead change, added to the plain update when ``with_plain``; with
-    ``learned_iters`` only the first that many iterations use the network."""
+    ``learned_iters`` only the first that many iterations use the network.
+    With ``pool`` > 1 the records also hold the flatness of the last ``pool``
+    iterations pooled (site_flatness_pooled)."""
     import torch
     R = drv.sm.n_replicas
     prev = np.full(R, np.inf)
@@ -559,6 +594,8 @@ def run_sites(drv: AlfBatch, n_iter: int, model=None, scale: float = 1.0, with_p
             rec["fallback"] = bad
         prev = rdev
         recs.append(rec)
+        if pool > 1:
+            rec["site_dev_pool"], rec["site_frac_pool"] = site_flatness_pooled(drv.sm, recs, pool, drv.T)
         drv.set_params(drv.params + delta)
     return recs
 

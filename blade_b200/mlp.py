@@ -126,8 +126,24 @@ class BF16MLP:
         return d
 
     def load(self, d: dict):
+        """Weights from ``state()``, or from a file that stores each weight
+        matrix as its BF16 bit patterns (``W{l}_bf16``)."""
+        d = weights_from_file_dict(d)
         assert list(d["sizes"]) == self.sizes
         for l in range(self.n_layers):
             self.W[l].copy_(self.torch.from_numpy(np.asarray(d[f"W{l}"], np.float32)))
             self.b[l].copy_(self.torch.from_numpy(np.asarray(d[f"b{l}"], np.float32)))
         self._sync_bf16()
+
+
+def weights_from_file_dict(d: dict) -> dict:
+    """``W{l}`` FP32 from ``W{l}_bf16`` (uint16 BF16 bit patterns) where only
+    the latter is present; other entries unchanged."""
+    out = dict(d)
+    l = 0
+    while f"W{l}_bf16" in out or f"W{l}" in out:
+        if f"W{l}" not in out:
+            bits = np.asarray(out[f"W{l}_bf16"], np.uint16).astype(np.uint32) << 16
+            out[f"W{l}"] = bits.view(np.float32)
+        l += 1
+    return out

@@ -248,6 +248,8 @@ def run_alf(args):
     from . import alf
     t0 = time.time()
     R, K = args.replicas, args.steps
+    if args.eval_only:
+        return eval_alf(args, t0)
     Xs, Ys, Xv, Yv, rounds = [], [], [], [], []
     if args.data_in:                                    # pairs made by an earlier "--data-out" run
         for f in sorted(os.listdir(args.data_in)):
@@ -317,26 +319,7 @@ def run_alf(args):
             xb = torch.from_numpy(np.ascontiguousarray(X_val[k:k + model.max_batch])).to(model.dev)
             preds.append(model.forward(xb).cpu().numpy())
         offline = alf.distance_to_flat(X_val, Y_val, W_val, np.concatenate(preds), K)
-    # evaluation on held-out systems: same systems, same MD seed, both methods
-    reps = flattening_replicas(range(50000, 50000 + R))
-    out = {}
-    modes = [m for m in args.eval_modes.split(",") if m]
-    for name in modes:  # plain | learned:<scale> | plain+learned:<scale> | learned_first:<iterations>
-        mdl = None if name == "plain" else model
-        arg = float(name.split(":")[1]) if ":" in name else 1.0
-        first = int(arg) if name.startswith("learned_first") else None
-        drv = alf.AlfBatch(reps, steps=K, seed=99)
-        recs = alf.run_sites(drv, args.eval_iters, mdl, scale=1.0 if first is not None else arg,
-                             with_plain=name.startswith("plain+"), learned_iters=first)
-        st = drv.status()
-        drv.close()
-        itf = alf.site_iterations_to_flat([(r["site_dev"], r["site_frac"]) for r in recs])
-        capped = np.where(itf > 0, itf, args.eval_iters + 1)
-        fb = [float(r["fallback"].mean()) for r in recs if r["fallback"] is not None]
-        out[name] = {"median_iterations_to_flat": float(np.median(capped)), "mean_iterations_to_flat": float(capped.mean()),
-                     "sites_flat": float((itf > 0).mean()),
-                     "site_dev_median_per_iteration": [round(float(np.median(r["site_dev"])), 3) for r in recs],
-                     "fallback_fraction": float(np.mean(fb)) if fb else None, "status": st}
+    out = evaluate_modes(args, model, R, K)
     line = {"config": f"learned flattening: {R} batched replicas of the 216-water box + 3 sites x 4 substituents "
                       f"(variants of one fragment), {K} steps (x 2 fs) per iteration",
             "flat_criterion": f"per site: max |end-state population - 1/4| <= {alf.FLAT_TOL}, "
@@ -351,6 +334,58 @@ def run_alf(args):
     print(json.dumps(line), flush=True)
 
 
+def evaluate_modes(args, model, R, K):
+    """Plain and learned flattening on held-out systems (same systems, same MD
+    seed): iterations until each site is first judged flat, per iteration
+    and, with --pool W, on the last W iterations pooled (alf.site_flatness_pooled)."""
+    from . import alf
+    reps = flattening_replicas(range(50000, 50000 + R))
+    out = {}
+    modes = [m for m in args.eval_modes.split(",") if m]
+    for name in modes:  # plain | learned:<scale> | plain+learned:<scale> | learned_first:<iterations>
+        mdl = None if name == "plain" else model
+        arg = float(name.split(":")[1]) if ":" in name else 1.0
+        first = int(arg) if name.startswith("learned_first") else None
+        drv = alf.AlfBatch(reps, steps=K, seed=99)
+        recs = alf.run_sites(drv, args.eval_iters, mdl, scale=1.0 if first is not None else arg,
+                             with_plain=name.startswith("plain+"), learned_iters=first, pool=args.pool)
+        st = drv.status()
+        drv.close()
+        itf = alf.site_iterations_to_flat([(r["site_dev"], r["site_frac"]) for r in recs])
+        capped = np.where(itf > 0, itf, args.eval_iters + 1)
+        fb = [float(r["fallback"].mean()) for r in recs if r["fallback"] is not None]
+        out[name] = {"median_iterations_to_flat": float(np.median(capped)), "mean_iterations_to_flat": float(capped.mean()),
+                     "sites_flat": float((itf > 0).mean()),
+                     "site_dev_median_per_iteration": [round(float(np.median(r["site_dev"])), 3) for r in recs],
+                     "fallback_fraction": float(np.mean(fb)) if fb else None, "status": st}
+        if args.pool > 1:
+            itp = alf.site_iterations_to_flat([(r["site_dev_pool"], r["site_frac_pool"]) for r in recs])
+            cp = np.where(itp > 0, itp, args.eval_iters + 1)
+            out[name]["pooled"] = {"window": args.pool, "median_iterations_to_flat": float(np.median(cp)),
+                                   "mean_iterations_to_flat": float(cp.mean()), "sites_flat": float((itp > 0).mean()),
+                                   "site_dev_median_per_iteration":
+                                       [round(float(np.median(r["site_dev_pool"])), 3) for r in recs]}
+    return out
+
+
+def eval_alf(args, t0):
+    """Evaluation only: the network of --model-in against the plain update."""
+    from . import alf
+    if not args.model_in:
+        raise SystemExit("--eval-only needs --model-in")
+    model = alf.new_model(seed=0)
+    model.load(dict(np.load(args.model_in)))
+    out = evaluate_modes(args, model, args.replicas, args.steps)
+    line = {"config": f"learned flattening, evaluation of {os.path.basename(args.model_in)}: {args.replicas} "
+                      f"batched replicas of the 216-water box + 3 sites x 4 substituents (variants of one "
+                      f"fragment), {args.steps} steps (x 2 fs) per iteration",
+            "flat_criterion": f"per site: max |end-state population - 1/4| <= {alf.FLAT_TOL}, "
+                              f">= {alf.END_FRAC_MIN} of samples at end states; per iteration, and pooled over "
+                              f"the last {args.pool} iterations reweighted to the current biases",
+            "eval_iterations": args.eval_iters, **out, "seconds_total": time.time() - t0}
+    print(json.dumps(line), flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["batch", "alf"])
@@ -358,6 +393,8 @@ def main(argv=None):
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--tune-sequential", action="store_true")
+    ap.add_argument("--pool", type=int, default=0, help="alf: also judge flatness on the last POOL iterations pooled")
+    ap.add_argument("--eval-only", action="store_true", help="alf: evaluate the network of --model-in only")
     ap.add_argument("--iters", type=int, default=60)
     ap.add_argument("--rounds", type=int, default=3)
     ap.add_argument("--eval-iters", type=int, default=30)

@@ -135,3 +135,37 @@ def test_committed_network_step_beats_plain_update():
     _, outs = mo.mlp_forward(X, Ws, bs)
     dist = alf.distance_to_flat(X, d["Y"], d["W"], outs[-1][1], int(d["samples"]))
     assert dist["network"] < 0.85 * dist["plain_update"], dist
+
+
+def test_pooled_flatness_reweights_end_states_exactly():
+    """Runs under different fixed biases pool to the populations of the last
+    biases: counts drawn as exact expectations from known end-state free
+    energies reweight to the same flatness as a run under the last biases."""
+    sm = alf._replica_map()
+    kT = alf.KB * 300.0
+    rng = np.random.default_rng(4)
+    G = rng.normal(0.0, 1.0, 13)                       # end-state free energies per block
+    recs = []
+    params = np.zeros(sm.n_params)
+    for t in range(4):
+        params = params.copy()
+        for k, g in enumerate(sm.sites):
+            params[sm.param_offset[k]:sm.param_offset[k] + len(g)] = rng.normal(0.0, 0.8, len(g))
+        he = np.zeros(13)
+        h1 = np.zeros((13, 32))
+        for k, g in enumerate(sm.sites):
+            b = params[sm.param_offset[k]:sm.param_offset[k] + len(g)]
+            p = np.exp(-(G[g] + b) / kT)
+            he[g] = 1e6 * p / p.sum()                      # all samples at end states
+            h1[g[0], 0] = 1e6
+        recs.append({"params": params, "he": he, "h1": h1})
+    dev_pool, frac_pool = alf.site_flatness_pooled(sm, recs, 4)
+    dev_last, frac_last = alf.site_flatness(sm, recs[-1]["h1"], recs[-1]["he"])
+    assert np.allclose(dev_pool, dev_last, atol=1e-9)
+    assert np.allclose(frac_pool, 1.0) and np.allclose(frac_last, 1.0)
+    same = [dict(r, params=recs[-1]["params"]) for r in recs]   # equal biases: plain sums
+    dev_same, _ = alf.site_flatness_pooled(sm, same, 4)
+    tot = sum(r["he"] for r in recs)
+    for k, g in enumerate(sm.sites):
+        c = tot[g]
+        assert dev_same[k] == pytest.approx(np.abs(c / c.sum() - 0.25).max(), abs=1e-12)
